@@ -1,0 +1,385 @@
+"""cuts_b200 -- B200 subgraph-isomorphism counting engine (Python host mirror).
+
+The engine is C++ host code and hand-written sm_100a CUDA kernels behind the
+C ABI in ``include/cuts_b200.h`` (``cuts_b200/lib/libcuts_b200.so``).  This
+module binds that ABI with ctypes and mirrors the reference's in-process API:
+
+* ``search(query_file, data_file, write_to_disk)``           -- host_funcs.cu:115
+* ``search_dfs_bfs_strategy(query_file, data_file, write_to_disk, trunks)``
+                                                              -- host_funcs.cu:39
+
+Both print the reference's progress lines and its result line
+``<data>,<query>,<ms>ms,<count>`` and return the count.  There is no CPU
+fallback: without the built library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libcuts_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "cuts")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "cuts_b200.h")
+
+OK = 0
+ERR_ARG, ERR_IO, ERR_PARSE, ERR_CUDA, ERR_NOMEM, ERR_QUERY, ERR_CAPACITY, ERR_LIMIT = range(1, 9)
+MAX_QUERY = 16
+FLAG_SYMMETRY_BREAK = 1
+FLAG_NO_CLOSED_FORM = 2
+ORDER_SCORE = 0
+ORDER_LEARNED = 1
+
+
+class CutsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cuts error {code}: {msg}")
+        self.code = code
+
+
+_lib: Optional[C.CDLL] = None
+
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_vp = C.c_void_p
+
+_SIGS = {
+    "cuts_last_error": (C.c_char_p, []),
+    "cuts_version": (C.c_char_p, []),
+    "cuts_hgraph_load": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "cuts_hgraph_gen_er": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.POINTER(_vp)]),
+    "cuts_hgraph_gen_chung_lu": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_double,
+                                           C.c_double, C.c_uint64, C.POINTER(_vp)]),
+    "cuts_hgraph_info": (C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_int), _u32p]),
+    "cuts_hgraph_csr": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cuts_hgraph_write": (C.c_int, [_vp, C.c_char_p]),
+    "cuts_graph_upload": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "cuts_hgraph_free": (None, [_vp]),
+    "cuts_gen_random_query": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _u32p, _u32p, _u32p]),
+    "cuts_graph_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    "cuts_graph_from_csr": (C.c_int, [C.c_uint32, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]),
+    "cuts_graph_info": (C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_int), _u32p]),
+    "cuts_graph_set_level_cap": (C.c_int, [_vp, C.c_uint64]),
+    "cuts_graph_free": (None, [_vp]),
+    "cuts_query_load": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "cuts_query_from_arcs": (C.c_int, [C.c_uint32, C.c_uint32, _u32p, _u32p, C.POINTER(_vp)]),
+    "cuts_query_info": (C.c_int, [_vp, _u32p, _u32p]),
+    "cuts_query_joins": (C.c_int, [_vp, _u32p, _u32p, _u32p, _u32p]),
+    "cuts_query_set_order": (C.c_int, [_vp, _u32p]),
+    "cuts_query_automorphisms": (C.c_int, [_vp, _u64p]),
+    "cuts_query_free": (None, [_vp]),
+    "cuts_count": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float)]),
+    "cuts_count_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float),
+                                _u64p, _u64p]),
+    "cuts_dump": (C.c_int, [_vp, _vp, C.c_char_p, _u64p]),
+    "cuts_search": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, _u64p,
+                              C.POINTER(C.c_float)]),
+    "cuts_count_batch": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.c_uint32, _u64p,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+}
+
+
+def lib() -> C.CDLL:
+    """The loaded engine library; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CutsError(ERR_IO, f"engine library missing: {LIB_PATH} (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise CutsError(rc, lib().cuts_last_error().decode())
+
+
+def _ptr(a: Optional[np.ndarray], t=_vp):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t) if t is not _vp else C.c_void_p(a.ctypes.data)
+
+
+# --------------------------------------------------------------------------
+# host graphs
+# --------------------------------------------------------------------------
+
+class HostGraph:
+    """Data graph in host memory (CSR built by the engine's loader)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str) -> "HostGraph":
+        h = _vp()
+        _check(lib().cuts_hgraph_load(path.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def erdos_renyi(cls, n: int, p: float, seed: int = 0) -> "HostGraph":
+        h = _vp()
+        _check(lib().cuts_hgraph_gen_er(n, p, seed, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def chung_lu(cls, n: int, m: int, gamma: float, wmin: float = 2.0, cap: float = 2e4,
+                 seed: int = 0) -> "HostGraph":
+        h = _vp()
+        _check(lib().cuts_hgraph_gen_chung_lu(n, m, gamma, wmin, cap, seed, C.byref(h)))
+        return cls(h)
+
+    def info(self) -> Tuple[int, int, bool, int]:
+        n, a, s, d = C.c_uint32(), C.c_uint64(), C.c_int(), C.c_uint32()
+        _check(lib().cuts_hgraph_info(self._h, C.byref(n), C.byref(a), C.byref(s), C.byref(d)))
+        return n.value, a.value, bool(s.value), d.value
+
+    @property
+    def n(self) -> int:
+        return self.info()[0]
+
+    def csr(self):
+        """(out_off, out_adj, in_off, in_adj); in_* are None when symmetric."""
+        n, arcs, sym, _ = self.info()
+        oo = np.zeros(n + 1, np.uint64)
+        oa = np.zeros(max(arcs, 1), np.uint32)
+        io = None if sym else np.zeros(n + 1, np.uint64)
+        ia = None if sym else np.zeros(max(arcs, 1), np.uint32)
+        _check(lib().cuts_hgraph_csr(self._h, _ptr(oo), _ptr(oa), _ptr(io), _ptr(ia)))
+        return oo, oa[:arcs], io, (ia[:arcs] if ia is not None else None)
+
+    def write(self, path: str) -> None:
+        _check(lib().cuts_hgraph_write(self._h, path.encode()))
+
+    def upload(self, device: int = 0) -> "Graph":
+        g = _vp()
+        _check(lib().cuts_graph_upload(self._h, device, C.byref(g)))
+        return Graph(g)
+
+    def close(self):
+        if self._h:
+            lib().cuts_hgraph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# queries
+# --------------------------------------------------------------------------
+
+class Query:
+    """Query graph with its matching order (score.cpp order by default)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str) -> "Query":
+        h = _vp()
+        _check(lib().cuts_query_load(path.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arcs(cls, k: int, arcs: Sequence[Tuple[int, int]]) -> "Query":
+        src = np.array([a for a, _ in arcs], np.uint32)
+        dst = np.array([b for _, b in arcs], np.uint32)
+        h = _vp()
+        _check(lib().cuts_query_from_arcs(k, len(arcs), _ptr(src, _u32p), _ptr(dst, _u32p),
+                                          C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edges(cls, k: int, edges: Sequence[Tuple[int, int]]) -> "Query":
+        """Undirected edges: both arcs of each edge."""
+        arcs = []
+        for a, b in edges:
+            arcs.append((a, b))
+            arcs.append((b, a))
+        return cls.from_arcs(k, arcs)
+
+    @property
+    def k(self) -> int:
+        k = C.c_uint32()
+        _check(lib().cuts_query_info(self._h, C.byref(k), None))
+        return k.value
+
+    @property
+    def order(self) -> List[int]:
+        k = self.k
+        o = np.zeros(k, np.uint32)
+        _check(lib().cuts_query_info(self._h, None, _ptr(o, _u32p)))
+        return [int(x) for x in o]
+
+    def set_order(self, order: Sequence[int]) -> None:
+        o = np.array(order, np.uint32)
+        _check(lib().cuts_query_set_order(self._h, _ptr(o, _u32p)))
+
+    def joins(self):
+        """P and C join lists per level position (graph.cpp:94-133)."""
+        k = self.k
+        po, co = np.zeros(k + 1, np.uint32), np.zeros(k + 1, np.uint32)
+        p, c = np.zeros(k * k + 1, np.uint32), np.zeros(k * k + 1, np.uint32)
+        _check(lib().cuts_query_joins(self._h, _ptr(po, _u32p), _ptr(p, _u32p), _ptr(co, _u32p),
+                                      _ptr(c, _u32p)))
+        P = [[int(x) for x in p[po[i]:po[i + 1]]] for i in range(k)]
+        Cl = [[int(x) for x in c[co[i]:co[i + 1]]] for i in range(k)]
+        return P, Cl
+
+    def automorphisms(self) -> int:
+        a = C.c_uint64()
+        _check(lib().cuts_query_automorphisms(self._h, C.byref(a)))
+        return a.value
+
+    def close(self):
+        if self._h:
+            lib().cuts_query_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# device graphs and counting
+# --------------------------------------------------------------------------
+
+@dataclass
+class CountResult:
+    count: int
+    ms: float
+    level_sizes: List[int] = field(default_factory=list)
+    launches: int = 0
+    chunks: int = 0
+    last_level_bytes: int = 0
+
+
+class Graph:
+    """Data graph resident on one GPU."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Graph":
+        h = _vp()
+        _check(lib().cuts_graph_load(path.encode(), device, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, n: int, out_off: np.ndarray, out_adj: np.ndarray,
+                 in_off: Optional[np.ndarray] = None, in_adj: Optional[np.ndarray] = None,
+                 device: int = 0) -> "Graph":
+        out_off = np.ascontiguousarray(out_off, np.uint64)
+        out_adj = np.ascontiguousarray(out_adj, np.uint32)
+        if in_off is not None:
+            in_off = np.ascontiguousarray(in_off, np.uint64)
+            in_adj = np.ascontiguousarray(in_adj, np.uint32)
+        h = _vp()
+        _check(lib().cuts_graph_from_csr(n, _ptr(out_off), _ptr(out_adj), _ptr(in_off),
+                                         _ptr(in_adj), device, C.byref(h)))
+        return cls(h)
+
+    def info(self) -> Tuple[int, int, bool, int]:
+        n, a, s, d = C.c_uint32(), C.c_uint64(), C.c_int(), C.c_uint32()
+        _check(lib().cuts_graph_info(self._h, C.byref(n), C.byref(a), C.byref(s), C.byref(d)))
+        return n.value, a.value, bool(s.value), d.value
+
+    def set_level_cap(self, entries: int) -> None:
+        _check(lib().cuts_graph_set_level_cap(self._h, entries))
+
+    def count(self, q: Query, chunks: int = 1, flags: int = 0, stats: bool = False,
+              alg_bytes: bool = False) -> CountResult:
+        cnt, ms = C.c_uint64(), C.c_float()
+        if not stats and not alg_bytes:
+            _check(lib().cuts_count(self._h, q._h, chunks, flags, C.byref(cnt), C.byref(ms)))
+            return CountResult(cnt.value, ms.value)
+        k = q.k
+        lv = np.zeros(k, np.uint64)
+        st = np.zeros(3, np.uint64)
+        st[2] = 1 if alg_bytes else 0
+        _check(lib().cuts_count_ex(self._h, q._h, chunks, flags, C.byref(cnt), C.byref(ms),
+                                   _ptr(lv, _u64p), _ptr(st, _u64p)))
+        return CountResult(cnt.value, ms.value, [int(x) for x in lv], int(st[0]), int(st[1]),
+                           int(st[2]))
+
+    def dump(self, q: Query, path: str) -> int:
+        n = C.c_uint64()
+        _check(lib().cuts_dump(self._h, q._h, path.encode(), C.byref(n)))
+        return n.value
+
+    def count_batch(self, queries: Sequence[Query], flags: int = 0):
+        nq = len(queries)
+        arr = (_vp * nq)(*[q._h for q in queries])
+        counts = np.zeros(nq, np.uint64)
+        status = (C.c_int * nq)()
+        ms = C.c_float()
+        _check(lib().cuts_count_batch(self._h, arr, nq, flags, _ptr(counts, _u64p), status,
+                                      C.byref(ms)))
+        return [int(x) for x in counts], list(status), ms.value
+
+    def close(self):
+        if self._h:
+            lib().cuts_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def search(query_file: str, data_file: str, write_to_disk: bool = False) -> int:
+    """Reference ``search()`` (host_funcs.cu:115-171)."""
+    cnt, ms = C.c_uint64(), C.c_float()
+    _check(lib().cuts_search(query_file.encode(), data_file.encode(), int(write_to_disk), 0,
+                             C.byref(cnt), C.byref(ms)))
+    return cnt.value
+
+
+def search_dfs_bfs_strategy(query_file: str, data_file: str, write_to_disk: bool,
+                            trunks: int) -> int:
+    """Reference ``search_dfs_bfs_strategy()`` (host_funcs.cu:39-114)."""
+    if trunks <= 0:
+        raise CutsError(ERR_ARG, "trunks must be >= 1")
+    cnt, ms = C.c_uint64(), C.c_float()
+    _check(lib().cuts_search(query_file.encode(), data_file.encode(), int(write_to_disk), trunks,
+                             C.byref(cnt), C.byref(ms)))
+    return cnt.value
+
+
+def random_query_arcs(k: int, p: float, seed: int) -> List[Tuple[int, int]]:
+    """Seeded random connected undirected query (both arcs per edge)."""
+    src = np.zeros(k * k, np.uint32)
+    dst = np.zeros(k * k, np.uint32)
+    na = C.c_uint32()
+    _check(lib().cuts_gen_random_query(k, p, seed, C.byref(na), _ptr(src, _u32p), _ptr(dst, _u32p)))
+    return [(int(src[i]), int(dst[i])) for i in range(na.value)]
+
+
+def write_query(path: str, k: int, arcs: Sequence[Tuple[int, int]]) -> None:
+    """Write a query in the reference text format."""
+    with open(path, "w") as f:
+        f.write(f"{k}\n")
+        for a, b in arcs:
+            f.write(f"{a}\t{b}\n")
+
+
+from .queries import NAMED_QUERIES, named_query_arcs  # noqa: E402

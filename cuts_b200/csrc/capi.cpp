@@ -1,0 +1,337 @@
+// capi.cpp -- the extern "C" surface declared in include/cuts_b200.h.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <memory>
+#include <new>
+
+#include "engine.hpp"
+#include "host.hpp"
+
+struct cuts_graph_s {
+    cuts::DeviceGraph *dev = nullptr;
+};
+struct cuts_query_s {
+    cuts::Query q;
+};
+struct cuts_hgraph_s {
+    cuts::HostGraph g;
+};
+
+using namespace cuts;
+
+#define GUARD(expr)                                                     \
+    try {                                                               \
+        return (expr);                                                  \
+    } catch (const std::bad_alloc &) {                                  \
+        return set_error(CUTS_ERR_NOMEM, "host allocation failed");     \
+    } catch (const std::exception &ex) {                                \
+        return set_error(CUTS_ERR_ARG, ex.what());                      \
+    }
+
+extern "C" {
+
+const char *cuts_last_error(void) { return last_error(); }
+const char *cuts_version(void) { return "cuts_b200 0.1"; }
+
+// ---- host graph ---------------------------------------------------------
+
+int cuts_hgraph_load(const char *path, cuts_hgraph *out) {
+    if (!path || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_hgraph_s>();
+        int rc = load_graph_text(path, h->g);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_hgraph_gen_er(uint32_t n, double p, uint64_t seed, cuts_hgraph *out) {
+    if (!out || p < 0 || p > 1) return set_error(CUTS_ERR_ARG, "bad argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_hgraph_s>();
+        gen_erdos_renyi(n, p, seed, h->g);
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_hgraph_gen_chung_lu(uint32_t n, uint64_t m, double gamma, double wmin, double cap,
+                             uint64_t seed, cuts_hgraph *out) {
+    if (!out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_hgraph_s>();
+        int rc = gen_chung_lu(n, m, gamma, wmin, cap, seed, h->g);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_hgraph_info(cuts_hgraph h, uint32_t *n, uint64_t *arcs, int *symmetric,
+                     uint32_t *max_degree) {
+    if (!h) return set_error(CUTS_ERR_ARG, "null graph");
+    if (n) *n = h->g.n;
+    if (arcs) *arcs = h->g.arcs;
+    if (symmetric) *symmetric = h->g.symmetric;
+    if (max_degree) *max_degree = h->g.max_degree();
+    return CUTS_OK;
+}
+
+int cuts_hgraph_csr(cuts_hgraph h, uint64_t *out_off, uint32_t *out_adj, uint64_t *in_off,
+                    uint32_t *in_adj) {
+    if (!h) return set_error(CUTS_ERR_ARG, "null graph");
+    const HostGraph &g = h->g;
+    if (out_off) std::memcpy(out_off, g.out_off.data(), sizeof(uint64_t) * (size_t(g.n) + 1));
+    if (out_adj && g.arcs) std::memcpy(out_adj, g.out_adj.data(), sizeof(uint32_t) * g.arcs);
+    if (!g.symmetric) {
+        if (in_off) std::memcpy(in_off, g.in_off.data(), sizeof(uint64_t) * (size_t(g.n) + 1));
+        if (in_adj && g.arcs) std::memcpy(in_adj, g.in_adj.data(), sizeof(uint32_t) * g.arcs);
+    }
+    return CUTS_OK;
+}
+
+int cuts_hgraph_write(cuts_hgraph h, const char *path) {
+    if (!h || !path) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(write_graph_text(path, h->g));
+}
+
+int cuts_graph_upload(cuts_hgraph h, int device, cuts_graph *out) {
+    if (!h || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto gh = std::make_unique<cuts_graph_s>();
+        int rc = device_graph_upload(h->g, device, &gh->dev);
+        if (rc) return rc;
+        *out = gh.release();
+        return CUTS_OK;
+    })());
+}
+
+void cuts_hgraph_free(cuts_hgraph h) { delete h; }
+
+int cuts_gen_random_query(uint32_t k, double p, uint64_t seed, uint32_t *narcs, uint32_t *src,
+                          uint32_t *dst) {
+    if (!narcs || !src || !dst || k == 0 || k > CUTS_MAX_QUERY)
+        return set_error(CUTS_ERR_ARG, "bad argument");
+    GUARD(([&]() {
+        std::vector<uint32_t> s, d;
+        gen_random_query(k, p, seed, s, d);
+        *narcs = uint32_t(s.size());
+        std::copy(s.begin(), s.end(), src);
+        std::copy(d.begin(), d.end(), dst);
+        return CUTS_OK;
+    })());
+}
+
+// ---- device graph ---------------------------------------------------------
+
+int cuts_graph_load(const char *path, int device, cuts_graph *out) {
+    if (!path || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        HostGraph g;
+        int rc = load_graph_text(path, g);
+        if (rc) return rc;
+        auto gh = std::make_unique<cuts_graph_s>();
+        rc = device_graph_upload(g, device, &gh->dev);
+        if (rc) return rc;
+        *out = gh.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj,
+                        const uint64_t *in_off, const uint32_t *in_adj, int device,
+                        cuts_graph *out) {
+    if (!out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        HostGraph g;
+        int rc = graph_from_csr(n, out_off, out_adj, in_off, in_adj, g);
+        if (rc) return rc;
+        auto gh = std::make_unique<cuts_graph_s>();
+        rc = device_graph_upload(g, device, &gh->dev);
+        if (rc) return rc;
+        *out = gh.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_graph_info(cuts_graph g, uint32_t *n, uint64_t *arcs, int *symmetric,
+                    uint32_t *max_degree) {
+    if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
+    if (n) *n = g->dev->n;
+    if (arcs) *arcs = g->dev->arcs;
+    if (symmetric) *symmetric = g->dev->symmetric;
+    if (max_degree) *max_degree = g->dev->max_deg;
+    return CUTS_OK;
+}
+
+int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries) {
+    if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
+    g->dev->level_cap_req = entries;
+    return CUTS_OK;
+}
+
+void cuts_graph_free(cuts_graph g) {
+    if (!g) return;
+    device_graph_free(g->dev);
+    delete g;
+}
+
+// ---- query ------------------------------------------------------------------
+
+int cuts_query_load(const char *path, cuts_query *out) {
+    if (!path || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto qh = std::make_unique<cuts_query_s>();
+        int rc = load_query_text(path, qh->q);
+        if (rc) return rc;
+        *out = qh.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_query_from_arcs(uint32_t k, uint32_t narcs, const uint32_t *src, const uint32_t *dst,
+                         cuts_query *out) {
+    if (!out || (narcs && (!src || !dst))) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto qh = std::make_unique<cuts_query_s>();
+        int rc = query_from_arcs(k, src, dst, narcs, qh->q);
+        if (rc) return rc;
+        *out = qh.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_query_info(cuts_query q, uint32_t *k, uint32_t *order) {
+    if (!q) return set_error(CUTS_ERR_ARG, "null query");
+    if (k) *k = q->q.k;
+    if (order) std::copy(q->q.order.begin(), q->q.order.end(), order);
+    return CUTS_OK;
+}
+
+int cuts_query_joins(cuts_query q, uint32_t *p_off, uint32_t *p, uint32_t *c_off, uint32_t *c) {
+    if (!q || !p_off || !p || !c_off || !c) return set_error(CUTS_ERR_ARG, "null argument");
+    const Query &Q = q->q;
+    p_off[0] = c_off[0] = 0;
+    for (uint32_t i = 0; i < Q.k; ++i) {
+        p_off[i + 1] = p_off[i];
+        for (uint32_t j : Q.P[i]) p[p_off[i + 1]++] = j;
+        c_off[i + 1] = c_off[i];
+        for (uint32_t j : Q.C[i]) c[c_off[i + 1]++] = j;
+    }
+    return CUTS_OK;
+}
+
+int cuts_query_set_order(cuts_query q, const uint32_t *order) {
+    if (!q || !order) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        Query tmp = q->q;
+        int rc = set_order(tmp, std::vector<uint32_t>(order, order + q->q.k));
+        if (rc) return rc;
+        q->q = std::move(tmp);
+        return CUTS_OK;
+    })());
+}
+
+int cuts_query_automorphisms(cuts_query q, uint64_t *count) {
+    if (!q || !count) return set_error(CUTS_ERR_ARG, "null argument");
+    *count = automorphism_count(q->q);
+    return CUTS_OK;
+}
+
+void cuts_query_free(cuts_query q) { delete q; }
+
+// ---- counting -----------------------------------------------------------------
+
+int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
+                  float *ms, uint64_t *level_sizes, uint64_t *stats) {
+    if (!g || !g->dev || !q) return set_error(CUTS_ERR_ARG, "null handle");
+    GUARD(([&]() {
+        CountResult r;
+        const bool want_bytes = stats && stats[2] != 0;
+        int rc = device_count(*g->dev, q->q, chunks, flags, want_bytes, r);
+        if (rc) return rc;
+        if (count) *count = r.count;
+        if (ms) *ms = r.ms;
+        if (level_sizes) std::copy(r.level_sizes, r.level_sizes + q->q.k, level_sizes);
+        if (stats) {
+            stats[0] = r.launches;
+            stats[1] = r.chunks;
+            stats[2] = r.last_level_bytes;
+        }
+        return CUTS_OK;
+    })());
+}
+
+int cuts_count(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
+               float *ms) {
+    return cuts_count_ex(g, q, chunks, flags, count, ms, nullptr, nullptr);
+}
+
+int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count) {
+    if (!g || !g->dev || !q || !path) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(device_dump(*g->dev, q->q, path, count));
+}
+
+static std::string base_name(const std::string &s) {
+    // common.cpp:19-26: the part after the last '/', or "" without one
+    size_t i = s.rfind('/');
+    return i == std::string::npos ? std::string() : s.substr(i + 1);
+}
+
+int cuts_search(const char *query_file, const char *data_file, int write_to_disk,
+                uint32_t trunks, uint64_t *count, float *ms) {
+    if (!query_file || !data_file) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        std::cout << "start loading graph file from disk to memory..." << std::endl;
+        Query q;
+        int rc = load_query_text(query_file, q);
+        if (rc) return rc;
+        HostGraph hg;
+        rc = load_graph_text(data_file, hg);
+        if (rc) return rc;
+        std::cout << "graph loading complete..." << std::endl;
+        std::cout << "start copying graph to gpu..." << std::endl;
+        DeviceGraph *dg = nullptr;
+        rc = device_graph_upload(hg, 0, &dg);
+        if (rc) return rc;
+        std::unique_ptr<DeviceGraph, void (*)(DeviceGraph *)> hold(dg, device_graph_free);
+        std::cout << (trunks ? "finish copying graph to gpu..." : "end copying graph to gpu...")
+                  << std::endl;
+        CountResult r;
+        rc = device_count(*dg, q, trunks ? trunks : 1, 0, false, r);
+        if (rc) return rc;
+        std::cout << base_name(data_file) << "," << base_name(query_file) << "," << r.ms << "ms,"
+                  << r.count << std::endl;
+        if (write_to_disk) {
+            std::cout << "start writting matching results to disk,ans.txt" << std::endl;
+            uint64_t lines = 0;
+            rc = device_dump(*dg, q, "ans.txt", &lines);
+            if (rc) return rc;
+            std::cout << "finish writting matching results to disk,ans.txt" << std::endl;
+        }
+        if (count) *count = r.count;
+        if (ms) *ms = r.ms;
+        return CUTS_OK;
+    })());
+}
+
+int cuts_count_batch(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                     uint64_t *counts, int *status, float *ms) {
+    if (!g || !g->dev || (nq && (!qs || !counts))) return set_error(CUTS_ERR_ARG, "null argument");
+    (void)flags; (void)status; (void)ms;
+    return set_error(CUTS_ERR_ARG, "batched counting not built yet");
+}
+
+}  // extern "C"

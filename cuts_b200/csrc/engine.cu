@@ -1,0 +1,794 @@
+// engine.cu -- device layout, level kernels and the chunked level driver.
+//
+// Method (the reference's, device_funcs.cu:267-405 and host_funcs.cu:
+// 39-171): a vertex-at-a-time join along the matching order.  Level L_0
+// holds the root candidates; level L_i holds (vertex, parent index) trie
+// entries, each extending one entry of L_{i-1} by a data vertex that lies
+// in every joined adjacency list, is not matched yet and passes the degree
+// signature.  The last level is counted, not stored.
+//
+// B200 layout of the work:
+//   * one warp per parent entry, parents handed out by a global work cursor
+//     in grains (work stealing across all SMs of a persistent grid);
+//   * the smallest joined list supplies the candidates (32 per step, one
+//     per lane); membership in the other lists is a lower-bound search;
+//   * survivors are placed with a warp ballot/popc into a per-warp shared
+//     staging buffer and flushed with one global atomic per buffer, so the
+//     next level is written in coalesced runs;
+//   * each stored entry carries an upper bound on its own child count (the
+//     shortest list it will join at the next level); a tile-sum + scan
+//     planner cuts every level into chunks whose bound fits the level's
+//     capacity, and the driver expands chunk by chunk depth-first, so the
+//     trie never exceeds the arena whatever the graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace cuts {
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return set_error(CUTS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr int kWarps = 8;       // warps per block in the level kernels
+constexpr int kOutBuf = 128;    // per-warp staged output entries
+constexpr uint32_t kTile = 256; // planner tile (parents)
+
+struct DevView {
+    const uint2 *out_info;
+    const uint2 *in_info;
+    const uint32_t *adj;
+    uint32_t n;
+};
+
+// Plan + level pointers, resident in device memory for the run.
+struct RunParams {
+    Plan plan;
+    uint32_t *vert[kMaxK];
+    uint32_t *par[kMaxK];
+    uint32_t *ub[kMaxK];
+};
+
+enum Mode { kExpand = 0, kCountMode = 1, kBytesMode = 2 };
+
+__device__ __forceinline__ uint32_t lbound(const uint32_t *__restrict__ a, uint32_t len,
+                                           uint32_t x) {
+    uint32_t lo = 0;
+    while (len > 0) {
+        uint32_t half = len >> 1;
+        if (__ldg(a + lo + half) < x) { lo += half + 1; len -= half + 1; }
+        else len = half;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool contains(const uint32_t *__restrict__ a, uint32_t len, uint32_t x) {
+    uint32_t p = lbound(a, len, x);
+    return p < len && __ldg(a + p) == x;
+}
+
+__device__ __forceinline__ uint32_t warp_min(uint32_t v) {
+    #pragma unroll
+    for (int s = 16; s; s >>= 1) v = min(v, __shfl_xor_sync(kFull, v, s));
+    return v;
+}
+
+// ---- level 0: signature scan (device_funcs.cu:267-279) ---------------
+__global__ void k_roots(DevView g, const RunParams *__restrict__ rp, uint32_t *__restrict__ n0) {
+    const Plan &P = rp->plan;
+    const uint32_t qin = P.lv[0].qin, qout = P.lv[0].qout;
+    // L_0 entries carry the child bound for level 1, whose joins all use
+    // position 0 (only needed when level 1 is stored, i.e. k >= 3)
+    const bool need_ub = P.k >= 3;
+    bool use_out = false, use_in = false;
+    if (P.k >= 2)
+        for (uint32_t t = 0; t < P.lv[1].nj; ++t) (P.lv[1].jdir[t] ? use_in : use_out) = true;
+    uint32_t *vert0 = rp->vert[0], *ub0 = rp->ub[0];
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < g.n; base += gridDim.x * blockDim.x) {
+        const uint32_t u = base + threadIdx.x;
+        bool ok = false;
+        uint32_t ub = UINT_MAX;
+        if (u < g.n) {
+            const uint2 o = g.out_info[u], i = g.in_info[u];
+            ok = o.y >= qout && i.y >= qin;
+            if (use_out) ub = min(ub, o.y);
+            if (use_in) ub = min(ub, i.y);
+        }
+        const unsigned m = __ballot_sync(kFull, ok);
+        if (m) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(n0, uint32_t(__popc(m)));
+            pos = __shfl_sync(kFull, pos, 0) + __popc(m & ((1u << lane) - 1));
+            if (ok) {
+                vert0[pos] = u;
+                if (need_ub) ub0[pos] = ub;
+            }
+        }
+    }
+}
+
+// ---- levels 1..k-1 -----------------------------------------------------
+// MODE kExpand: write L_lvl from parents [pa, pb) of L_{lvl-1}.
+// MODE kCountMode: last level, accumulate the count.
+// MODE kBytesMode: accumulate the algorithmic bytes of the last level.
+template <int MODE>
+__global__ void __launch_bounds__(kWarps * 32)
+k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, uint32_t pb,
+        uint32_t grain, uint32_t *__restrict__ cursor, uint32_t *__restrict__ out_n,
+        uint32_t out_cap, uint32_t *__restrict__ err, unsigned long long *__restrict__ acc) {
+    __shared__ LevelPlan sL, sN;
+    __shared__ uint32_t *s_vert[kMaxK];
+    __shared__ uint32_t *s_par[kMaxK];
+    __shared__ uint32_t s_k, s_sym;
+    __shared__ uint32_t wm[kWarps][kMaxK];
+    __shared__ uint32_t joff[kWarps][kMaxJ], jdeg[kWarps][kMaxJ];
+    __shared__ uint32_t ob_v[MODE == kExpand ? kWarps : 1][kOutBuf];
+    __shared__ uint32_t ob_p[MODE == kExpand ? kWarps : 1][kOutBuf];
+    __shared__ uint32_t ob_u[MODE == kExpand ? kWarps : 1][kOutBuf];
+
+    {
+        const uint32_t words = sizeof(LevelPlan) / 4;
+        const uint32_t *srcL = reinterpret_cast<const uint32_t *>(&rp->plan.lv[lvl]);
+        uint32_t *dL = reinterpret_cast<uint32_t *>(&sL);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dL[i] = srcL[i];
+        const uint32_t nl = lvl + 1 < rp->plan.k ? lvl + 1 : lvl;
+        const uint32_t *srcN = reinterpret_cast<const uint32_t *>(&rp->plan.lv[nl]);
+        uint32_t *dN = reinterpret_cast<uint32_t *>(&sN);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dN[i] = srcN[i];
+        if (threadIdx.x < kMaxK) {
+            s_vert[threadIdx.x] = rp->vert[threadIdx.x];
+            s_par[threadIdx.x] = rp->par[threadIdx.x];
+        }
+        if (threadIdx.x == 0) { s_k = rp->plan.k; s_sym = rp->plan.symmetric; }
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lanemask_lt = (1u << lane) - 1;
+    uint32_t *my_m = wm[warp];
+    const uint32_t k = s_k;
+    const bool sym = s_sym != 0;
+    const bool need_ub = MODE == kExpand && lvl + 2 < k;
+    uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
+    uint32_t *out_p = MODE == kExpand ? rp->par[lvl] : nullptr;
+    uint32_t *out_u = MODE == kExpand ? rp->ub[lvl] : nullptr;
+    // next-level joins on the child itself (position lvl) bound its children
+    bool ub_out = false, ub_in = false;
+    if (need_ub)
+        for (uint32_t t = 0; t < sN.nj; ++t)
+            if (sN.jpos[t] == lvl) (sN.jdir[t] ? ub_in : ub_out) = true;
+    const uint32_t nj = sL.nj;
+    const bool check_sig = sL.check_sig != 0;
+    const bool load_info = check_sig || ub_out || ub_in;
+
+    uint32_t cached_q = kFull;  // lane 0: L_{lvl-2} index whose path is in my_m[0..lvl-2]
+    uint32_t obn = 0;           // staged outputs (warp-uniform)
+    unsigned long long local = 0;
+    const uint32_t total = pb - pa;
+
+    auto flush = [&]() {
+        if constexpr (MODE != kExpand) return;
+        __syncwarp();
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(out_n, obn);
+        base = __shfl_sync(kFull, base, 0);
+        if (base + obn <= out_cap && base + obn >= base) {
+            for (uint32_t i = lane; i < obn; i += 32) {
+                out_v[base + i] = ob_v[warp][i];
+                out_p[base + i] = ob_p[warp][i];
+                if (need_ub) out_u[base + i] = ob_u[warp][i];
+            }
+        } else if (lane == 0) {
+            atomicOr(err, 1u);
+        }
+        obn = 0;
+        __syncwarp();
+    };
+
+    while (true) {
+        uint32_t start = 0;
+        if (lane == 0) start = atomicAdd(cursor, grain);
+        start = __shfl_sync(kFull, start, 0);
+        if (start >= total) break;
+        const uint32_t end = min(start + grain, total);
+        for (uint32_t pi = start; pi < end; ++pi) {
+            const uint32_t p = pa + pi;
+            // rebuild the parent's partial match (device_funcs.cu:39-55),
+            // reusing the ancestors shared with the previous parent
+            if (lane == 0) {
+                my_m[lvl - 1] = s_vert[lvl - 1][p];
+                if (lvl >= 2) {
+                    uint32_t q = s_par[lvl - 1][p];
+                    if (q != cached_q) {
+                        cached_q = q;
+                        for (int j = int(lvl) - 2; j >= 0; --j) {
+                            my_m[j] = s_vert[j][q];
+                            if (j > 0) q = s_par[j][q];
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+
+            // joined lists; the shortest supplies the candidates
+            uint32_t my_deg = kFull, my_off = 0;
+            if (uint32_t(lane) < nj) {
+                const uint32_t u = my_m[sL.jpos[lane]];
+                const uint2 inf = sL.jdir[lane] ? g.in_info[u] : g.out_info[u];
+                my_off = inf.x;
+                my_deg = inf.y;
+                joff[warp][lane] = my_off;
+                jdeg[warp][lane] = my_deg;
+            }
+            uint32_t bd = my_deg, bl = uint32_t(lane);
+            #pragma unroll
+            for (int s = 16; s; s >>= 1) {
+                const uint32_t od = __shfl_xor_sync(kFull, bd, s), ol = __shfl_xor_sync(kFull, bl, s);
+                if (od < bd || (od == bd && ol < bl)) { bd = od; bl = ol; }
+            }
+            if (nj == 0) { __syncwarp(); continue; }  // unreachable for validated orders
+            const uint32_t tmin = bl, mdeg = bd;
+            const uint32_t moff = __shfl_sync(kFull, my_off, int(tmin));
+            __syncwarp();
+
+            if constexpr (MODE == kBytesMode) {
+                if (lane == 0) {
+                    unsigned long long b = 8;
+                    for (uint32_t t = 0; t < nj; ++t) b += 4ull * jdeg[warp][t] + 8;
+                    local += b;
+                }
+                __syncwarp();
+                continue;
+            }
+
+            // symmetry-breaking window [lo, hi) on the candidate value
+            uint32_t lo = 0, hi = kFull;
+            for (uint32_t msk = sL.gt_mask; msk; msk &= msk - 1) lo = max(lo, my_m[__ffs(msk) - 1] + 1);
+            for (uint32_t msk = sL.lt_mask; msk; msk &= msk - 1) hi = min(hi, my_m[__ffs(msk) - 1]);
+            const uint32_t *mlist = g.adj + moff;
+            const uint32_t s0 = lo ? lbound(mlist, mdeg, lo) : 0;
+            const uint32_t e0 = hi != kFull ? lbound(mlist, mdeg, hi) : mdeg;
+
+            if (MODE == kCountMode && sL.closed_form) {  // uniform branch
+                // one joined list, no signature: every list element in the
+                // window except the already-matched vertices extends
+                if (s0 < e0) {
+                    bool hit = false;
+                    if (uint32_t(lane) < lvl) {
+                        const uint32_t mj = my_m[lane];
+                        hit = mj >= lo && mj < hi && contains(mlist, mdeg, mj);
+                    }
+                    const uint32_t sub = __popc(__ballot_sync(kFull, hit));
+                    if (lane == 0) local += (e0 - s0) - sub;
+                }
+                __syncwarp();
+                continue;
+            }
+
+            uint32_t ubp = kFull;
+            if (need_ub) {
+                uint32_t d = kFull;
+                if (uint32_t(lane) < sN.nj && sN.jpos[lane] < lvl) {
+                    const uint32_t u = my_m[sN.jpos[lane]];
+                    d = (sN.jdir[lane] ? g.in_info[u] : g.out_info[u]).y;
+                }
+                ubp = warp_min(d);
+            }
+
+            for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
+                const uint32_t x = x0 + lane;
+                bool ok = x < e0;
+                const uint32_t c = ok ? __ldg(mlist + x) : 0;
+                if (ok)
+                    for (uint32_t j = 0; j < lvl; ++j)
+                        if (c == my_m[j]) { ok = false; break; }
+                uint2 co = make_uint2(0, 0), ci = make_uint2(0, 0);
+                if (ok && load_info) {
+                    co = g.out_info[c];
+                    ci = sym ? co : g.in_info[c];
+                }
+                if (ok && check_sig) ok = ci.y >= sL.qin && co.y >= sL.qout;
+                if (ok)
+                    for (uint32_t t = 0; t < nj; ++t) {
+                        if (t == tmin) continue;
+                        if (!contains(g.adj + joff[warp][t], jdeg[warp][t], c)) { ok = false; break; }
+                    }
+                if constexpr (MODE == kCountMode) {
+                    local += ok;
+                } else {
+                    uint32_t ub = ubp;
+                    if (ub_out) ub = min(ub, co.y);
+                    if (ub_in) ub = min(ub, ci.y);
+                    const unsigned m = __ballot_sync(kFull, ok);
+                    const uint32_t nn = __popc(m);
+                    if (obn + nn > uint32_t(kOutBuf)) flush();
+                    if (ok) {
+                        const uint32_t r = obn + __popc(m & lanemask_lt);
+                        ob_v[warp][r] = c;
+                        ob_p[warp][r] = p;
+                        ob_u[warp][r] = ub;
+                    }
+                    obn += nn;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if constexpr (MODE == kExpand) {
+        if (obn) flush();
+    } else {
+        #pragma unroll
+        for (int s = 16; s; s >>= 1) local += __shfl_xor_sync(kFull, local, s);
+        if (lane == 0 && local) atomicAdd(acc, local);
+    }
+}
+
+// ---- chunk planner ------------------------------------------------------
+// Tile sums of the child bounds of parents [pa, pb).
+__global__ void k_tile_sums(const uint32_t *__restrict__ ub, uint32_t pa, uint32_t pb,
+                            uint32_t tile, uint64_t *__restrict__ tsum,
+                            unsigned long long *__restrict__ tmax) {
+    __shared__ unsigned long long red[32];
+    const uint32_t ntiles = (pb - pa + tile - 1) / tile;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t b = pa + t * tile, e = min(b + tile, pb);
+        unsigned long long s = 0;
+        for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) s += ub[i];
+        #pragma unroll
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0;
+            #pragma unroll
+            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+            if (threadIdx.x == 0) {
+                tsum[t] = s;
+                atomicMax(tmax, s);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Chunk boundaries (tile indices): tile t opens a chunk when
+// floor(prefix(t) / cap_eff) differs from tile t-1's; with cap_eff = cap -
+// (max tile sum) every chunk's bound sum stays within cap.  One block.
+__global__ void __launch_bounds__(1024)
+k_plan(const uint64_t *__restrict__ tsum, uint32_t ntiles, unsigned long long cap_eff,
+       uint32_t *__restrict__ bounds, uint32_t *__restrict__ nb_out) {
+    __shared__ unsigned long long ws[32];
+    __shared__ uint32_t wf[32];
+    __shared__ unsigned long long carry;
+    __shared__ uint32_t nb;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) { carry = 0; nb = 0; }
+    __syncthreads();
+    for (uint32_t base = 0; base < ntiles; base += blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
+        const unsigned long long v = t < ntiles ? tsum[t] : 0;
+        // inclusive block scan of v
+        unsigned long long x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long w = lane < int(blockDim.x / 32) ? ws[lane] : 0;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, w, o);
+                if (lane >= o) w += y;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long incl = x + (warp ? ws[warp - 1] : 0) + carry;
+        const unsigned long long excl = incl - v;
+        bool flag = false;
+        if (t < ntiles) {
+            if (t == 0) flag = true;
+            else {
+                const unsigned long long prev_excl = excl - tsum[t - 1];
+                flag = (excl / cap_eff) != (prev_excl / cap_eff);
+            }
+        }
+        // ordered compaction of the flags
+        const unsigned m = __ballot_sync(kFull, flag);
+        if (lane == 0) wf[warp] = __popc(m);
+        __syncthreads();
+        uint32_t before = 0, tot = 0;
+        for (int w = 0; w < int(blockDim.x / 32); ++w) {
+            if (w < warp) before += wf[w];
+            tot += wf[w];
+        }
+        if (flag) bounds[nb + before + __popc(m & ((1u << lane) - 1))] = t;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        if (threadIdx.x == 0) nb += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bounds[nb] = ntiles;
+        *nb_out = nb;
+    }
+}
+
+int g_num_sms = 0;
+int g_level_blocks[3] = {0, 0, 0};
+
+int launch_geometry() {
+    if (g_num_sms) return CUTS_OK;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    int b = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level<kExpand>, kWarps * 32, 0));
+    g_level_blocks[kExpand] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level<kCountMode>, kWarps * 32, 0));
+    g_level_blocks[kCountMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level<kBytesMode>, kWarps * 32, 0));
+    g_level_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
+    return CUTS_OK;
+}
+
+// u32 scratch slots
+enum : int { kSlotN0 = 0, kSlotErr = 1, kSlotNb = 2, kSlotOut = 8, kSlotCursor = 32, kSlots = 64 };
+
+}  // namespace
+
+// ---- upload -------------------------------------------------------------
+
+int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
+    *out = nullptr;
+    CK(cudaSetDevice(device));
+    const uint32_t n = hg.n;
+    // padded layout: every list starts at a multiple of 4 words
+    auto build = [&](bool in_dir, std::vector<uint2> &info, uint64_t &words) {
+        info.resize(n);
+        uint64_t w = 0;
+        for (uint32_t v = 0; v < n; ++v) {
+            const uint32_t d = in_dir ? hg.in_deg(v) : hg.out_deg(v);
+            info[v] = make_uint2(uint32_t(w), d);
+            w += (uint64_t(d) + 3) & ~uint64_t(3);
+        }
+        words = w;
+    };
+    std::vector<uint2> oinfo, iinfo;
+    uint64_t owords = 0, iwords = 0;
+    build(false, oinfo, owords);
+    if (!hg.symmetric) build(true, iinfo, iwords);
+    const uint64_t total_words = owords + iwords;
+    if (total_words >= (uint64_t(1) << 32))
+        return set_error(CUTS_ERR_LIMIT, "padded adjacency exceeds 2^32 words");
+    if (!hg.symmetric)
+        for (auto &x : iinfo) x.x += uint32_t(owords);
+    std::vector<uint32_t> adj(std::max<uint64_t>(total_words, 4), 0xffffffffu);
+    #pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t v = 0; v < int64_t(n); ++v) {
+        std::memcpy(adj.data() + oinfo[v].x, hg.out_list(uint32_t(v)), sizeof(uint32_t) * oinfo[v].y);
+        if (!hg.symmetric)
+            std::memcpy(adj.data() + iinfo[v].x, hg.in_list(uint32_t(v)), sizeof(uint32_t) * iinfo[v].y);
+    }
+    auto *g = new DeviceGraph();
+    g->device = device;
+    g->n = n;
+    g->arcs = hg.arcs;
+    g->symmetric = hg.symmetric;
+    g->max_deg = hg.max_degree();
+    g->adj_words = adj.size();
+    auto fail = [&](cudaError_t e, const char *what) {
+        device_graph_free(g);
+        return set_error(CUTS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking))) return fail(e, "stream");
+    if ((e = cudaMalloc(&g->out_info, sizeof(uint2) * std::max<uint32_t>(n, 1)))) return fail(e, "cudaMalloc info");
+    if (!hg.symmetric) {
+        if ((e = cudaMalloc(&g->in_info, sizeof(uint2) * std::max<uint32_t>(n, 1)))) return fail(e, "cudaMalloc info");
+    } else {
+        g->in_info = g->out_info;
+    }
+    if ((e = cudaMalloc(&g->adj, sizeof(uint32_t) * adj.size()))) return fail(e, "cudaMalloc adjacency");
+    if (n) {
+        if ((e = cudaMemcpyAsync(g->out_info, oinfo.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, g->stream)))
+            return fail(e, "upload");
+        if (!hg.symmetric &&
+            (e = cudaMemcpyAsync(g->in_info, iinfo.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, g->stream)))
+            return fail(e, "upload");
+    }
+    if ((e = cudaMemcpyAsync(g->adj, adj.data(), sizeof(uint32_t) * adj.size(), cudaMemcpyHostToDevice, g->stream)))
+        return fail(e, "upload");
+    if ((e = cudaMalloc(&g->d_u32, sizeof(uint32_t) * kSlots))) return fail(e, "scratch");
+    if ((e = cudaMalloc(&g->d_u64, sizeof(unsigned long long) * 8))) return fail(e, "scratch");
+    if ((e = cudaMalloc(&g->d_plan, sizeof(RunParams)))) return fail(e, "scratch");
+    if ((e = cudaMallocHost(&g->h_u32, sizeof(uint32_t) * kSlots))) return fail(e, "pinned");
+    if ((e = cudaMallocHost(&g->h_u64, sizeof(unsigned long long) * 8))) return fail(e, "pinned");
+    if ((e = cudaMallocHost(&g->h_plan, sizeof(RunParams)))) return fail(e, "pinned");
+    if ((e = cudaEventCreate(&g->ev0)) || (e = cudaEventCreate(&g->ev1))) return fail(e, "event");
+    if ((e = cudaStreamSynchronize(g->stream))) return fail(e, "upload sync");
+    // default arena: proportional to the graph, within [256 MB, 64 GB] and
+    // at most 60% of the free memory
+    size_t freeb = 0, totb = 0;
+    cudaMemGetInfo(&freeb, &totb);
+    double want = 384.0 * double(hg.arcs) + 64.0 * n;
+    want = std::max(want, 256.0 * (1 << 20));
+    want = std::min(want, 64.0 * (1ull << 30));
+    want = std::min(want, 0.6 * double(freeb));
+    g->arena_bytes = size_t(want);
+    *out = g;
+    return CUTS_OK;
+}
+
+void device_graph_free(DeviceGraph *g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->in_info && g->in_info != g->out_info) cudaFree(g->in_info);
+    cudaFree(g->out_info);
+    cudaFree(g->adj);
+    cudaFree(g->arena);
+    cudaFree(g->d_u32);
+    cudaFree(g->d_u64);
+    cudaFree(g->d_plan);
+    cudaFree(g->d_tiles);
+    cudaFree(g->d_bounds);
+    cudaFreeHost(g->h_u32);
+    cudaFreeHost(g->h_u64);
+    cudaFreeHost(g->h_plan);
+    cudaFreeHost(g->h_bounds);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+// ---- driver -----------------------------------------------------------------
+
+namespace {
+
+struct Run {
+    DeviceGraph &g;
+    DevView view;
+    RunParams *hp;        // pinned host copy
+    RunParams *dp;        // device copy
+    uint32_t k;
+    uint64_t cap;         // entries per stored level >= 1
+    uint32_t grain;
+    bool bytes_mode;
+    CountResult &res;
+
+    int sync() {
+        CK(cudaStreamSynchronize(g.stream));
+        return CUTS_OK;
+    }
+
+    int ensure_tiles(size_t ntiles) {
+        if (ntiles + 1 <= g.tiles_cap) return CUTS_OK;
+        size_t nc = std::max(ntiles + 1, g.tiles_cap * 2);
+        cudaFree(g.d_tiles);
+        cudaFree(g.d_bounds);
+        cudaFreeHost(g.h_bounds);
+        g.d_tiles = nullptr; g.d_bounds = nullptr; g.h_bounds = nullptr; g.tiles_cap = 0;
+        CK(cudaMalloc(&g.d_tiles, sizeof(uint64_t) * nc));
+        CK(cudaMalloc(&g.d_bounds, sizeof(uint32_t) * nc));
+        CK(cudaMallocHost(&g.h_bounds, sizeof(uint32_t) * nc));
+        g.tiles_cap = nc;
+        return CUTS_OK;
+    }
+
+    // Splits parents [pa, pb) of L_{lvl-1} into chunks whose child bounds fit cap.
+    int plan_chunks(uint32_t lvl, uint32_t pa, uint32_t pb, std::vector<uint32_t> &cuts) {
+        cuts.clear();
+        if (uint64_t(pb - pa) * g.max_deg <= cap) { cuts = {pa, pb}; return CUTS_OK; }
+        uint64_t tile = std::min<uint64_t>(kTile, cap / (2ull * std::max<uint32_t>(g.max_deg, 1)));
+        if (tile == 0)
+            return set_error(CUTS_ERR_CAPACITY, "level capacity below twice the maximum degree");
+        const uint32_t ntiles = uint32_t((uint64_t(pb - pa) + tile - 1) / tile);
+        int rc = ensure_tiles(ntiles);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(g.d_u64 + 1, 0, sizeof(unsigned long long), g.stream));
+        const uint32_t blocks = std::min<uint32_t>(ntiles, uint32_t(g_num_sms) * 16);
+        k_tile_sums<<<blocks, 256, 0, g.stream>>>(hp->ub[lvl - 1], pa, pb, uint32_t(tile), g.d_tiles,
+                                                 g.d_u64 + 1);
+        CK(cudaMemcpyAsync(g.h_u64 + 1, g.d_u64 + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
+        res.launches++;
+        int r2 = sync();
+        if (r2) return r2;
+        const unsigned long long tmax = g.h_u64[1];
+        const unsigned long long cap_eff = cap - tmax;
+        k_plan<<<1, 1024, 0, g.stream>>>(g.d_tiles, ntiles, cap_eff, g.d_bounds, g.d_u32 + kSlotNb);
+        res.launches++;
+        CK(cudaMemcpyAsync(g.h_u32 + kSlotNb, g.d_u32 + kSlotNb, sizeof(uint32_t), cudaMemcpyDeviceToHost, g.stream));
+        r2 = sync();
+        if (r2) return r2;
+        const uint32_t nb = g.h_u32[kSlotNb];
+        CK(cudaMemcpyAsync(g.h_bounds, g.d_bounds, sizeof(uint32_t) * (nb + 1), cudaMemcpyDeviceToHost, g.stream));
+        r2 = sync();
+        if (r2) return r2;
+        for (uint32_t c = 0; c <= nb; ++c)
+            cuts.push_back(uint32_t(std::min<uint64_t>(pa + uint64_t(g.h_bounds[c]) * tile, pb)));
+        return CUTS_OK;
+    }
+
+    int launch_level(int mode, uint32_t lvl, uint32_t pa, uint32_t pb) {
+        CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
+        uint32_t *out_n = g.d_u32 + kSlotOut + lvl;
+        if (mode == kExpand) CK(cudaMemsetAsync(out_n, 0, sizeof(uint32_t), g.stream));
+        const uint32_t work = pb - pa;
+        const uint32_t warps_needed = (work + grain - 1) / grain;
+        uint32_t blocks = std::min<uint32_t>(uint32_t(g_level_blocks[mode]),
+                                             (warps_needed + kWarps - 1) / kWarps);
+        blocks = std::max<uint32_t>(blocks, 1);
+        if (mode == kExpand)
+            k_level<kExpand><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
+                g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, g.d_u64);
+        else if (mode == kCountMode)
+            k_level<kCountMode><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
+                g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, g.d_u64);
+        else
+            k_level<kBytesMode><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
+                g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, g.d_u64 + 2);
+        CK(cudaGetLastError());
+        res.launches++;
+        return CUTS_OK;
+    }
+
+    // Expands parents [pa, pb) of L_{lvl-1}, depth first by chunks.
+    int expand(uint32_t lvl, uint32_t pa, uint32_t pb) {
+        if (pb <= pa) return CUTS_OK;
+        if (lvl + 1 == k) {
+            int rc = launch_level(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
+            return rc;
+        }
+        std::vector<uint32_t> cuts;
+        int rc = plan_chunks(lvl, pa, pb, cuts);
+        if (rc) return rc;
+        for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+            const uint32_t a = cuts[c], b = cuts[c + 1];
+            if (b <= a) continue;
+            rc = launch_level(kExpand, lvl, a, b);
+            if (rc) return rc;
+            res.chunks++;
+            CK(cudaMemcpyAsync(g.h_u32 + kSlotOut + lvl, g.d_u32 + kSlotOut + lvl, sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, g.stream));
+            CK(cudaMemcpyAsync(g.h_u32 + kSlotErr, g.d_u32 + kSlotErr, sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, g.stream));
+            rc = sync();
+            if (rc) return rc;
+            const uint32_t nout = g.h_u32[kSlotOut + lvl];
+            if (g.h_u32[kSlotErr] || nout > cap)
+                return set_error(CUTS_ERR_CAPACITY, "level " + std::to_string(lvl) + " overflowed its capacity");
+            res.level_sizes[lvl] += nout;
+            rc = expand(lvl + 1, 0, nout);
+            if (rc) return rc;
+        }
+        return CUTS_OK;
+    }
+};
+
+}  // namespace
+
+int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags, bool want_bytes,
+                 CountResult &res) {
+    res = CountResult();
+    if (chunks == 0) return set_error(CUTS_ERR_ARG, "chunks must be >= 1");
+    CK(cudaSetDevice(g.device));
+    int rc = launch_geometry();
+    if (rc) return rc;
+    const uint32_t k = q.k;
+    RunParams *hp = static_cast<RunParams *>(g.h_plan);
+    std::memset(hp, 0, sizeof(RunParams));
+    rc = build_plan(q, g.symmetric, flags, hp->plan);
+    if (rc) return rc;
+    // arena: L_0 (vert, ub) with n entries, then L_1..L_{k-2} (vert, par, ub)
+    if (!g.arena) {
+        cudaError_t e = cudaMalloc(&g.arena, g.arena_bytes);
+        if (e != cudaSuccess) {
+            g.arena = nullptr;
+            return set_error(CUTS_ERR_NOMEM, "arena allocation failed: " + std::string(cudaGetErrorString(e)));
+        }
+    }
+    const uint64_t n = g.n;
+    const uint64_t l0_bytes = ((8 * n + 255) / 256) * 256 + 256;
+    uint64_t cap = 0;
+    if (g.arena_bytes < l0_bytes) return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level");
+    if (k >= 3) {
+        if (g.arena_bytes <= l0_bytes) return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level");
+        cap = (g.arena_bytes - l0_bytes) / (12ull * (k - 2));
+        cap = std::min<uint64_t>(cap, (1ull << 31) - 64);
+        if (g.level_cap_req) cap = std::min<uint64_t>(cap, g.level_cap_req);
+        cap &= ~uint64_t(63);
+        if (cap < 2ull * std::max<uint32_t>(g.max_deg, 1) || cap == 0)
+            return set_error(CUTS_ERR_CAPACITY, "level capacity below twice the maximum degree");
+    }
+    char *base = static_cast<char *>(g.arena);
+    hp->vert[0] = reinterpret_cast<uint32_t *>(base);
+    hp->ub[0] = reinterpret_cast<uint32_t *>(base + ((4 * n + 255) / 256) * 256);
+    hp->par[0] = nullptr;
+    char *cur = base + l0_bytes;
+    for (uint32_t i = 1; i + 1 < k; ++i) {
+        hp->vert[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
+        hp->par[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
+        hp->ub[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
+    }
+    RunParams *dp = static_cast<RunParams *>(g.d_plan);
+    CK(cudaMemcpyAsync(dp, hp, sizeof(RunParams), cudaMemcpyHostToDevice, g.stream));
+
+    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
+    CK(cudaEventRecord(g.ev0, g.stream));
+    CK(cudaMemsetAsync(g.d_u32, 0, sizeof(uint32_t) * kSlots, g.stream));
+    CK(cudaMemsetAsync(g.d_u64, 0, sizeof(unsigned long long) * 8, g.stream));
+    uint32_t n0 = 0;
+    if (g.n) {
+        const uint32_t threads = 256;
+        const uint32_t blocks = std::min<uint32_t>((g.n + threads - 1) / threads, uint32_t(g_num_sms) * 8);
+        k_roots<<<blocks, threads, 0, g.stream>>>(run.view, dp, g.d_u32 + kSlotN0);
+        CK(cudaGetLastError());
+        res.launches++;
+        CK(cudaMemcpyAsync(g.h_u32 + kSlotN0, g.d_u32 + kSlotN0, sizeof(uint32_t), cudaMemcpyDeviceToHost, g.stream));
+        rc = run.sync();
+        if (rc) return rc;
+        n0 = g.h_u32[kSlotN0];
+    }
+    res.level_sizes[0] = n0;
+    if (k >= 2 && n0 > 0) {
+        // root slices, as the reference's trunks (host_funcs.cu:66-72)
+        const uint32_t slice = uint32_t((uint64_t(n0) - 1) / chunks + 1);
+        for (uint32_t s = 0; s < chunks; ++s) {
+            const uint64_t a = uint64_t(s) * slice;
+            if (a >= n0) break;
+            const uint32_t b = uint32_t(std::min<uint64_t>(a + slice, n0));
+            rc = run.expand(1, uint32_t(a), b);
+            if (rc) return rc;
+        }
+    }
+    CK(cudaEventRecord(g.ev1, g.stream));
+    CK(cudaMemcpyAsync(g.h_u64, g.d_u64, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
+    rc = run.sync();
+    if (rc) return rc;
+    CK(cudaEventElapsedTime(&res.ms, g.ev0, g.ev1));
+    const uint64_t raw = k >= 2 ? uint64_t(g.h_u64[0]) : 0;
+    res.level_sizes[k - 1] = k >= 2 ? raw : n0;
+    res.count = raw * hp->plan.aut;
+    if (want_bytes && k >= 2 && n0 > 0) {
+        // untimed second pass: algorithmic bytes of the last-level kernel
+        CountResult tmp;
+        Run r2{g, run.view, hp, dp, k, cap, 4, true, tmp};
+        CK(cudaMemsetAsync(g.d_u64 + 2, 0, sizeof(unsigned long long), g.stream));
+        const uint32_t slice = uint32_t((uint64_t(n0) - 1) / chunks + 1);
+        for (uint32_t s = 0; s < chunks; ++s) {
+            const uint64_t a = uint64_t(s) * slice;
+            if (a >= n0) break;
+            rc = r2.expand(1, uint32_t(a), uint32_t(std::min<uint64_t>(a + slice, n0)));
+            if (rc) return rc;
+        }
+        CK(cudaMemcpyAsync(g.h_u64 + 2, g.d_u64 + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
+        rc = r2.sync();
+        if (rc) return rc;
+        res.last_level_bytes = g.h_u64[2];
+    }
+    return CUTS_OK;
+}
+
+int device_dump(DeviceGraph &, const Query &, const char *, uint64_t *) {
+    return set_error(CUTS_ERR_ARG, "dump not built yet");
+}
+
+}  // namespace cuts

@@ -1,0 +1,301 @@
+// query.cpp -- query graphs, the greedy score order, symmetry conditions and
+// the per-level plan the kernels execute.
+#include <algorithm>
+#include <functional>
+
+#include "host.hpp"
+
+namespace cuts {
+
+bool Query::has_arc(uint32_t a, uint32_t b) const {
+    return std::binary_search(out[a].begin(), out[a].end(), b);
+}
+
+bool Query::loop_free() const {
+    for (uint32_t v = 0; v < k; ++v)
+        if (self_loop(v)) return false;
+    return true;
+}
+
+bool Query::weakly_connected() const {
+    if (k == 0) return false;
+    std::vector<char> seen(k, 0);
+    std::vector<uint32_t> st{0};
+    seen[0] = 1;
+    uint32_t cnt = 1;
+    while (!st.empty()) {
+        uint32_t v = st.back();
+        st.pop_back();
+        for (auto *lst : {&out[v], &in[v]})
+            for (uint32_t w : *lst)
+                if (!seen[w]) { seen[w] = 1; ++cnt; st.push_back(w); }
+    }
+    return cnt == k;
+}
+
+int query_from_arcs(uint32_t k, const uint32_t *src, const uint32_t *dst, uint32_t narcs,
+                    Query &q) {
+    if (k == 0) return set_error(CUTS_ERR_QUERY, "query has no vertices");
+    if (k > uint32_t(kMaxK))
+        return set_error(CUTS_ERR_QUERY, "query has more than " + std::to_string(kMaxK) + " vertices");
+    q = Query();
+    q.k = k;
+    q.out.assign(k, {});
+    q.in.assign(k, {});
+    for (uint32_t i = 0; i < narcs; ++i) {
+        if (src[i] >= k || dst[i] >= k) return set_error(CUTS_ERR_ARG, "query arc out of range");
+        q.out[src[i]].push_back(dst[i]);
+        q.in[dst[i]].push_back(src[i]);
+    }
+    for (uint32_t v = 0; v < k; ++v) {
+        for (auto *l : {&q.out[v], &q.in[v]}) {
+            std::sort(l->begin(), l->end());
+            l->erase(std::unique(l->begin(), l->end()), l->end());
+        }
+    }
+    if (k > 1 && !q.weakly_connected())
+        return set_error(CUTS_ERR_QUERY,
+                         "query is not connected (the reference's order repeats a vertex there)");
+    std::vector<uint32_t> order;
+    int rc = score_order(q, order);
+    if (rc) return rc;
+    return set_order(q, order);
+}
+
+int load_query_text(const std::string &path, Query &q) {
+    HostGraph g;
+    int rc = load_graph_text(path, g);
+    if (rc) return rc;
+    if (g.n > uint32_t(kMaxK))
+        return set_error(CUTS_ERR_QUERY, "query has more than " + std::to_string(kMaxK) + " vertices");
+    std::vector<uint32_t> s, d;
+    for (uint32_t u = 0; u < g.n; ++u)
+        for (uint64_t a = g.out_off[u]; a < g.out_off[u + 1]; ++a) {
+            s.push_back(u);
+            d.push_back(g.out_adj[a]);
+        }
+    return query_from_arcs(g.n, s.data(), d.data(), uint32_t(s.size()), q);
+}
+
+// ---- score order: graph.cpp:62-93, score.cpp:18-99 -------------------
+
+static bool in_prefix(uint32_t v, const std::vector<uint32_t> &sel, size_t len) {
+    for (size_t i = 0; i < len; ++i)
+        if (sel[i] == v) return true;
+    return false;
+}
+
+// arcs between v and the ordered set, counted from both sides (score.cpp:18-35)
+static uint32_t score1(const Query &q, const std::vector<uint32_t> &sel, size_t len, uint32_t v) {
+    uint32_t s = 0;
+    for (size_t i = 0; i < len; ++i) s += q.has_arc(sel[i], v);
+    for (uint32_t w : q.out[v]) s += in_prefix(w, sel, len);
+    return s;
+}
+// v's out-neighbours among the unordered out-neighbours of the ordered set (score.cpp:36-54)
+static uint32_t score2(const Query &q, const std::vector<uint32_t> &sel, size_t len, uint32_t v) {
+    std::vector<char> mark(q.k, 0);
+    for (size_t i = 0; i < len; ++i)
+        for (uint32_t w : q.out[sel[i]])
+            if (!in_prefix(w, sel, len)) mark[w] = 1;
+    uint32_t s = 0;
+    for (uint32_t w = 0; w < q.k; ++w) s += mark[w] && q.has_arc(v, w);
+    return s;
+}
+// v's out-neighbours outside the ordered set and its out-neighbourhood (score.cpp:56-80)
+static uint32_t score3(const Query &q, const std::vector<uint32_t> &sel, size_t len, uint32_t v) {
+    std::vector<char> reach(q.k, 0);
+    for (size_t i = 0; i < len; ++i) {
+        reach[sel[i]] = 1;
+        for (uint32_t w : q.out[sel[i]]) reach[w] = 1;
+    }
+    uint32_t s = 0;
+    for (uint32_t w = 0; w < q.k; ++w) s += !reach[w] && q.has_arc(v, w);
+    return s;
+}
+
+int score_order(const Query &q, std::vector<uint32_t> &order) {
+    order.assign(q.k, 0);
+    uint32_t maxd = 0, idx = 0;
+    for (uint32_t v = 0; v < q.k; ++v)
+        if (maxd < q.out[v].size()) { maxd = uint32_t(q.out[v].size()); idx = v; }
+    order[0] = idx;
+    for (size_t ins = 1; ins < q.k; ++ins) {
+        uint32_t b1 = 0, b2 = 0, b3 = 0;
+        for (uint32_t v = 0; v < q.k; ++v) {
+            if (in_prefix(v, order, ins)) continue;
+            uint32_t s1 = score1(q, order, ins, v), s2 = score2(q, order, ins, v),
+                     s3 = score3(q, order, ins, v);
+            // strict lexicographic '>' (score.cpp:81-99): lowest id wins ties
+            if (s1 > b1 || (s1 == b1 && (s2 > b2 || (s2 == b2 && s3 > b3)))) {
+                b1 = s1; b2 = s2; b3 = s3; idx = v;
+            }
+        }
+        order[ins] = idx;
+    }
+    return CUTS_OK;
+}
+
+int set_order(Query &q, const std::vector<uint32_t> &order) {
+    if (order.size() != q.k) return set_error(CUTS_ERR_ARG, "order length != k");
+    std::vector<char> seen(q.k, 0);
+    for (uint32_t v : order) {
+        if (v >= q.k || seen[v]) return set_error(CUTS_ERR_ARG, "order is not a permutation");
+        seen[v] = 1;
+    }
+    q.order = order;
+    q.P.assign(q.k, {});
+    q.C.assign(q.k, {});
+    for (uint32_t i = 1; i < q.k; ++i) {
+        uint32_t v = order[i];
+        for (uint32_t j = 0; j < i; ++j) {
+            uint32_t t = order[j];
+            if (q.has_arc(v, t)) q.C[i].push_back(j);   // arc v -> order[j]
+            if (q.has_arc(t, v)) q.P[i].push_back(j);   // arc order[j] -> v
+        }
+        if (q.P[i].empty() && q.C[i].empty())
+            return set_error(CUTS_ERR_QUERY, "order position " + std::to_string(i) +
+                                                 " has no arc to an earlier position");
+    }
+    return CUTS_OK;
+}
+
+// ---- automorphisms ------------------------------------------------------
+
+// Finds one arc-preserving permutation with perm[fixed[i]] = fixed[i] and
+// perm[v] = w, by backtracking over vertices in id order.
+static bool find_automorphism(const Query &q, const std::vector<uint32_t> &fixed, uint32_t v,
+                              uint32_t w) {
+    const uint32_t k = q.k;
+    std::vector<int> img(k, -1), used(k, 0);
+    for (uint32_t f : fixed) { img[f] = int(f); used[f] = 1; }
+    if (img[v] >= 0 && img[v] != int(w)) return false;
+    if (img[v] < 0) {
+        if (used[w]) return false;
+        img[v] = int(w);
+        used[w] = 1;
+    }
+    auto consistent = [&](uint32_t a) {
+        uint32_t fa = uint32_t(img[a]);
+        if (q.out[a].size() != q.out[fa].size() || q.in[a].size() != q.in[fa].size()) return false;
+        for (uint32_t b = 0; b < k; ++b) {
+            if (img[b] < 0) continue;
+            uint32_t fb = uint32_t(img[b]);
+            if (q.has_arc(a, b) != q.has_arc(fa, fb)) return false;
+            if (q.has_arc(b, a) != q.has_arc(fb, fa)) return false;
+        }
+        return true;
+    };
+    for (uint32_t a = 0; a < k; ++a)
+        if (img[a] >= 0 && !consistent(a)) return false;
+    std::function<bool(uint32_t)> rec = [&](uint32_t a) -> bool {
+        if (a == k) return true;
+        if (img[a] >= 0) return rec(a + 1);
+        for (uint32_t c = 0; c < k; ++c) {
+            if (used[c]) continue;
+            img[a] = int(c);
+            used[c] = 1;
+            if (consistent(a) && rec(a + 1)) return true;
+            used[c] = 0;
+            img[a] = -1;
+        }
+        return false;
+    };
+    return rec(0);
+}
+
+// Stabiliser chain: repeatedly take the earliest-ordered vertex with a
+// nontrivial orbit under the current stabiliser, require f(v) < f(w) for the
+// rest of its orbit, then fix v.  |Aut| = product of the orbit sizes.
+static void stabiliser_chain(const Query &q, std::vector<std::pair<uint32_t, uint32_t>> *conds,
+                             uint64_t *aut) {
+    std::vector<uint32_t> fixed;
+    uint64_t total = 1;
+    std::vector<uint32_t> by_pos = q.order.empty() ? std::vector<uint32_t>() : q.order;
+    if (by_pos.empty())
+        for (uint32_t v = 0; v < q.k; ++v) by_pos.push_back(v);
+    while (true) {
+        bool any = false;
+        for (uint32_t v : by_pos) {
+            if (std::find(fixed.begin(), fixed.end(), v) != fixed.end()) continue;
+            std::vector<uint32_t> orbit;
+            for (uint32_t w = 0; w < q.k; ++w)
+                if (w == v || find_automorphism(q, fixed, v, w)) orbit.push_back(w);
+            if (orbit.size() > 1) {
+                for (uint32_t w : orbit)
+                    if (w != v && conds) conds->push_back({v, w});
+                total *= orbit.size();
+                fixed.push_back(v);
+                any = true;
+                break;
+            }
+        }
+        if (!any) break;
+    }
+    if (aut) *aut = total;
+}
+
+std::vector<std::pair<uint32_t, uint32_t>> symmetry_conditions(const Query &q) {
+    std::vector<std::pair<uint32_t, uint32_t>> c;
+    stabiliser_chain(q, &c, nullptr);
+    return c;
+}
+
+uint64_t automorphism_count(const Query &q) {
+    uint64_t a = 1;
+    stabiliser_chain(q, nullptr, &a);
+    return a;
+}
+
+// ---- plan ---------------------------------------------------------------
+
+int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) {
+    plan = Plan();
+    plan.k = q.k;
+    plan.symmetric = data_symmetric;
+    plan.aut = 1;
+    const uint32_t k = q.k;
+    for (uint32_t i = 0; i < k; ++i) {
+        LevelPlan &L = plan.lv[i];
+        const uint32_t v = q.order[i];
+        L.qin = uint32_t(q.in[v].size());
+        L.qout = uint32_t(q.out[v].size());
+        uint32_t nj = 0;
+        auto add = [&](uint32_t pos, uint32_t dir) {
+            if (data_symmetric) dir = 0;  // in-list == out-list: one list per position
+            for (uint32_t t = 0; t < nj; ++t)
+                if (L.jpos[t] == pos && L.jdir[t] == dir) return;
+            L.jpos[nj] = uint8_t(pos);
+            L.jdir[nj] = uint8_t(dir);
+            ++nj;
+        };
+        if (i > 0) {
+            for (uint32_t j : q.P[i]) add(j, 0);  // candidate in out-list of m_j
+            for (uint32_t j : q.C[i]) add(j, 1);  // candidate in in-list of m_j
+        }
+        L.nj = nj;
+        // At the last level every arc of order[k-1] is a join, so a
+        // candidate that passes the joins and injectivity already has the
+        // degrees the signature asks for -- unless the query vertex has a
+        // self-loop, which the joins never check but the signature counts.
+        L.check_sig = (i + 1 < k) || q.self_loop(v);
+        L.closed_form = (k >= 2 && i + 1 == k && nj == 1 && !L.check_sig &&
+                         !(flags & CUTS_FLAG_NO_CLOSED_FORM));
+    }
+    if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && k >= 2) {
+        std::vector<uint32_t> pos(k);
+        for (uint32_t i = 0; i < k; ++i) pos[q.order[i]] = i;
+        std::vector<std::pair<uint32_t, uint32_t>> conds;
+        uint64_t aut = 1;
+        stabiliser_chain(q, &conds, &aut);
+        for (auto &c : conds) {  // f(a) < f(b)
+            uint32_t pa = pos[c.first], pb = pos[c.second];
+            if (pb > pa) plan.lv[pb].gt_mask |= 1u << pa;
+            else plan.lv[pa].lt_mask |= 1u << pb;
+        }
+        plan.aut = aut;
+    }
+    return CUTS_OK;
+}
+
+}  // namespace cuts

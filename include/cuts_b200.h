@@ -1,0 +1,178 @@
+/*
+ * cuts_b200.h -- C ABI of the B200 subgraph-isomorphism counting engine.
+ *
+ * Plain C types only (no C++ or torch types).  Every function returns an
+ * int status (CUTS_OK == 0); on failure cuts_last_error() returns a
+ * thread-local message.  Handles own their device memory; the caller frees
+ * them.  A handle is not thread-safe; use one per host thread.
+ *
+ * Each entry point names the reference (cuTS) interface it replaces.
+ */
+#ifndef CUTS_B200_H
+#define CUTS_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUTS_OK 0
+#define CUTS_ERR_ARG 1        /* invalid argument */
+#define CUTS_ERR_IO 2         /* file cannot be opened / read */
+#define CUTS_ERR_PARSE 3      /* malformed graph text */
+#define CUTS_ERR_CUDA 4       /* CUDA runtime error */
+#define CUTS_ERR_NOMEM 5      /* host or device allocation failed */
+#define CUTS_ERR_QUERY 6      /* query unsupported (disconnected, too large) */
+#define CUTS_ERR_CAPACITY 7   /* a level exceeds its capacity */
+#define CUTS_ERR_LIMIT 8      /* graph exceeds a size limit of the layout */
+
+#define CUTS_MAX_QUERY 16     /* query vertices (reference: QUERY_NODES 12) */
+
+/* cuts_count flags */
+#define CUTS_FLAG_SYMMETRY_BREAK 1u  /* count one embedding per automorphism
+                                        orbit and scale by |Aut(Q)| (exact;
+                                        query must be loop-free) */
+#define CUTS_FLAG_NO_CLOSED_FORM 2u  /* enumerate the last level even when a
+                                        closed form exists */
+
+/* order modes for cuts_plan */
+#define CUTS_ORDER_SCORE 0    /* greedy score order (score.cpp) */
+#define CUTS_ORDER_LEARNED 1  /* learned cost model, score order fallback */
+
+typedef struct cuts_graph_s *cuts_graph;   /* data graph resident on one GPU */
+typedef struct cuts_query_s *cuts_query;   /* query graph + matching order */
+typedef struct cuts_hgraph_s *cuts_hgraph; /* data graph in host memory (CSR) */
+
+const char *cuts_last_error(void);
+const char *cuts_version(void);
+
+/* ---- host graph: loader, generators, writer ------------------------ */
+
+/* Parse a graph file into a host CSR.  Replaces file_reader (util.cpp:
+ * 19-52) and the CSR build of Graph::Graph (graph.cpp:18-61). */
+int cuts_hgraph_load(const char *path, cuts_hgraph *out);
+/* Seeded undirected Erdos-Renyi G(n, p), both arcs per edge.  No reference
+ * counterpart (the reference reads SNAP files only). */
+int cuts_hgraph_gen_er(uint32_t n, double p, uint64_t seed, cuts_hgraph *out);
+/* Seeded undirected Chung-Lu graph with exactly m distinct edges, weights
+ * min(cap, wmin * U^(-1/(gamma-1))).  No reference counterpart. */
+int cuts_hgraph_gen_chung_lu(uint32_t n, uint64_t m, double gamma, double wmin, double cap,
+                             uint64_t seed, cuts_hgraph *out);
+int cuts_hgraph_info(cuts_hgraph h, uint32_t *n, uint64_t *arcs, int *symmetric,
+                     uint32_t *max_degree);
+/* Copy the CSR out (arrays sized n+1 / arcs; in_* ignored when symmetric). */
+int cuts_hgraph_csr(cuts_hgraph h, uint64_t *out_off, uint32_t *out_adj, uint64_t *in_off,
+                    uint32_t *in_adj);
+/* Write the reference text format (line 1 = V, then "s<TAB>t"). */
+int cuts_hgraph_write(cuts_hgraph h, const char *path);
+/* Make a host graph resident on `device` (the host graph stays valid).
+ * Replaces malloc_graph_gpu_memory (gpu_memory_allocation.cu:26-37). */
+int cuts_graph_upload(cuts_hgraph h, int device, cuts_graph *out);
+void cuts_hgraph_free(cuts_hgraph h);
+
+/* Seeded random connected undirected query: a random spanning tree plus each
+ * other pair with probability p.  Writes both arcs of each edge into
+ * src/dst (capacity k*k each) and their number into *narcs.  No reference
+ * counterpart. */
+int cuts_gen_random_query(uint32_t k, double p, uint64_t seed, uint32_t *narcs, uint32_t *src,
+                          uint32_t *dst);
+
+/* ---- data graph --------------------------------------------------- */
+
+/* Load a graph file (line 1 = V, then "s<TAB>t" arcs) and make it resident
+ * on `device`.  Replaces Graph::Graph(1, file) (graph.cpp:18-61, util.cpp:
+ * 19-52) followed by malloc_graph_gpu_memory (gpu_memory_allocation.cu:
+ * 26-37). */
+int cuts_graph_load(const char *path, int device, cuts_graph *out);
+
+/* The same from host CSR arrays (offsets n+1, sorted duplicate-free lists).
+ * in_off/in_adj NULL means the graph is symmetric (in-lists == out-lists).
+ * Replaces malloc_graph_gpu_memory (gpu_memory_allocation.cu:26-37). */
+int cuts_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj,
+                        const uint64_t *in_off, const uint32_t *in_adj, int device,
+                        cuts_graph *out);
+
+/* n, distinct arcs, 1 if symmetric, maximum list length. */
+int cuts_graph_info(cuts_graph g, uint32_t *n, uint64_t *arcs, int *symmetric,
+                    uint32_t *max_degree);
+
+/* Cap (in entries) of each intermediate trie level; 0 = automatic (sized
+ * from free device memory).  Smaller caps force more chunks.  Replaces the
+ * fixed GPU_TABLE_LIMIT (common.h:25, gpu_memory_allocation.cu:56-59). */
+int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries);
+
+void cuts_graph_free(cuts_graph g);
+
+/* ---- query graph -------------------------------------------------- */
+
+/* Load a query file and compute the score order.  Replaces
+ * Graph::Graph(0, file) (graph.cpp:18-61) + sort_search_order
+ * (graph.cpp:62-134). */
+int cuts_query_load(const char *path, cuts_query *out);
+
+/* Query from an arc list (k vertices, arcs as given; add both arcs for an
+ * undirected edge).  Duplicates collapse, as in util.cpp:46-47. */
+int cuts_query_from_arcs(uint32_t k, uint32_t narcs, const uint32_t *src,
+                         const uint32_t *dst, cuts_query *out);
+
+/* Number of query vertices and the current order (k entries). */
+int cuts_query_info(cuts_query q, uint32_t *k, uint32_t *order);
+
+/* P/C join lists of the current order over level positions (graph.cpp:
+ * 94-133): p_off/c_off have k+1 entries, p/c at most k*k. */
+int cuts_query_joins(cuts_query q, uint32_t *p_off, uint32_t *p, uint32_t *c_off,
+                     uint32_t *c);
+
+/* Replace the order (a permutation whose every prefix is connected). */
+int cuts_query_set_order(cuts_query q, const uint32_t *order);
+
+/* |Aut(Q)| (arc-preserving permutations). */
+int cuts_query_automorphisms(cuts_query q, uint64_t *count);
+
+void cuts_query_free(cuts_query q);
+
+/* ---- counting ----------------------------------------------------- */
+
+/* Count embeddings of q in g (reference semantics: injective, arc
+ * preserving, degree signature filter).  chunks >= 1 splits the root level
+ * into that many slices, as the reference's trunks argument does; memory
+ * driven chunking is automatic on top of it.  *ms = device time from the
+ * first kernel to the last, as the reference times it.  Replaces search()
+ * (host_funcs.cu:115-171) and search_dfs_bfs_strategy() (host_funcs.cu:
+ * 39-114) after the graphs are resident. */
+int cuts_count(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+               uint64_t *count, float *ms);
+
+/* As cuts_count, and also reports per-level sizes |L_0|..|L_{k-1}|
+ * (level_sizes has k entries; with CUTS_FLAG_SYMMETRY_BREAK they are the
+ * constrained sizes) and launch statistics: stats[0] = kernels launched,
+ * stats[1] = chunks expanded, stats[2] = bytes of algorithmic traffic of
+ * the last-level kernel (only when stats[2] is nonzero on entry: an extra
+ * untimed pass computes it). */
+int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                  uint64_t *count, float *ms, uint64_t *level_sizes, uint64_t *stats);
+
+/* Write every embedding to `path` in the reference's ans.txt line format
+ * "(q,d)(q,d)..." in matching order (util.cpp:53-74).  Returns the number
+ * of lines in *count.  Line order is unspecified, as in the reference. */
+int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count);
+
+/* Reference in-process API (host_funcs.h:21-25): load both files, make the
+ * data graph resident, count, print "<data>,<query>,<ms>ms,<count>" and,
+ * when write_to_disk != 0, write ans.txt in the working directory.
+ * trunks == 0 runs search(); trunks >= 1 runs search_dfs_bfs_strategy(). */
+int cuts_search(const char *query_file, const char *data_file, int write_to_disk,
+                uint32_t trunks, uint64_t *count, float *ms);
+
+/* ---- batched counting -------------------------------------------- */
+
+/* Count nq queries against one resident graph in one persistent launch.
+ * counts[nq] receives exact per-query counts; status[nq] (may be NULL)
+ * receives 0 or a CUTS_ERR_* code per query. */
+int cuts_count_batch(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                     uint64_t *counts, int *status, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,181 @@
+"""Engine counts vs the CPU oracle on the same seeded inputs (bit-exact).
+
+Every case compares the total count and, where the order is the same, every
+per-level table size |L_i| (which pins the per-level semantics, not only the
+final number).
+"""
+import numpy as np
+import pytest
+
+import cuts_b200 as cb
+from oracle import oracle as O
+from tests.helpers import csr_from_arcs, directed_er, oracle_graph_from_host
+
+pytestmark = pytest.mark.gpu
+
+NAMED = ["triangle", "4-cycle", "5-cycle", "house", "4-clique+pendant", "3-prism", "6-cycle"]
+
+
+@pytest.fixture(scope="module")
+def er2k():
+    h = cb.HostGraph.erdos_renyi(2000, 10.0 / 1999, seed=3)
+    return h, h.upload(0), oracle_graph_from_host(h)
+
+
+@pytest.fixture(scope="module")
+def cl5k():
+    h = cb.HostGraph.chung_lu(5000, 30000, 2.1, 2.0, 400.0, seed=5)
+    return h, h.upload(0), oracle_graph_from_host(h)
+
+
+def _check(g, od, k, arcs, flags=0, chunks=1, levels=True):
+    q = cb.Query.from_arcs(k, arcs)
+    oq = O.Graph.from_arcs(k, arcs)
+    cnt, lv, _ = O.count(od, oq, q.order)
+    r = g.count(q, chunks=chunks, flags=flags, stats=True)
+    assert r.count == cnt
+    if levels:
+        assert r.level_sizes == lv
+    return cnt
+
+
+@pytest.mark.parametrize("name", NAMED)
+def test_named_er(er2k, name):
+    h, g, od = er2k
+    k, arcs = cb.named_query_arcs(name)
+    _check(g, od, k, arcs)
+
+
+@pytest.mark.parametrize("name", ["triangle", "4-cycle", "house", "4-clique+pendant"])
+def test_named_power_law(cl5k, name):
+    h, g, od = cl5k
+    k, arcs = cb.named_query_arcs(name)
+    _check(g, od, k, arcs)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_queries(er2k, seed):
+    h, g, od = er2k
+    k = 4 + seed % 4
+    arcs = cb.random_query_arcs(k, 0.3, seed)
+    _check(g, od, k, arcs)
+
+
+@pytest.mark.parametrize("name", ["4-cycle", "house", "5-cycle"])
+def test_forced_chunking(er2k, name):
+    """A tiny level capacity forces the planner to cut every level."""
+    h, g, od = er2k
+    k, arcs = cb.named_query_arcs(name)
+    g.set_level_cap(1024)
+    try:
+        q = cb.Query.from_arcs(k, arcs)
+        r = g.count(q, stats=True)
+        cnt, lv, _ = O.count(od, O.Graph.from_arcs(k, arcs), q.order)
+        assert r.count == cnt and r.level_sizes == lv
+        assert r.chunks > k  # really chunked
+    finally:
+        g.set_level_cap(0)
+
+
+@pytest.mark.parametrize("trunks", [1, 2, 4, 7])
+def test_trunks(er2k, trunks):
+    h, g, od = er2k
+    k, arcs = cb.named_query_arcs("house")
+    _check(g, od, k, arcs, chunks=trunks)
+
+
+@pytest.mark.parametrize("name", NAMED)
+def test_symmetry_breaking(cl5k, name):
+    h, g, od = cl5k
+    k, arcs = cb.named_query_arcs(name)
+    q = cb.Query.from_arcs(k, arcs)
+    cnt, _, _ = O.count(od, O.Graph.from_arcs(k, arcs), q.order)
+    assert g.count(q, flags=cb.FLAG_SYMMETRY_BREAK).count == cnt
+
+
+@pytest.mark.parametrize("name", ["triangle", "4-clique+pendant", "5-cycle"])
+def test_no_closed_form(er2k, name):
+    h, g, od = er2k
+    k, arcs = cb.named_query_arcs(name)
+    _check(g, od, k, arcs, flags=cb.FLAG_NO_CLOSED_FORM)
+
+
+def test_directed_graph_and_queries():
+    n, src, dst = directed_er(1500, 14.0, seed=11)
+    oo, oa, io, ia, s, d = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo, oa, io, ia)
+    assert not g.info()[2]
+    od = O.Graph.from_arrays(n, s, d)
+    rng = np.random.default_rng(0)
+    for t in range(10):
+        k = 3 + t % 4
+        und = cb.random_query_arcs(k, 0.5, 100 + t)
+        # orient: keep each arc with prob 0.7 but keep the query connected
+        arcs = [a for a in und if rng.random() < 0.7 or a[0] < a[1]]
+        _check(g, od, k, arcs)
+
+
+def test_self_loops():
+    """Self-loops in the data graph count in degrees; a query self-loop is
+    only a signature constraint, as in the reference."""
+    n = 300
+    h = cb.HostGraph.erdos_renyi(n, 0.05, seed=2)
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(oo.astype(np.int64)))
+    loops = np.arange(0, n, 3, dtype=np.uint32)
+    src = np.concatenate([src, loops])
+    dst = np.concatenate([oa, loops])
+    oo2, oa2, io2, ia2, s, d = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo2, oa2, io2, ia2)
+    od = O.Graph.from_arrays(n, s, d)
+    k, arcs = cb.named_query_arcs("triangle")
+    _check(g, od, k, arcs)
+    _check(g, od, 3, arcs + [(2, 2)])
+    _check(g, od, 3, arcs + [(0, 0)])
+
+
+def test_small_queries_and_empty():
+    h = cb.HostGraph.erdos_renyi(500, 0.02, seed=9)
+    g = h.upload(0)
+    od = oracle_graph_from_host(h)
+    # one vertex: the reference reports 0 (count only added at iter == k-1 >= 1)
+    q1 = cb.Query.from_arcs(1, [])
+    assert g.count(q1).count == 0
+    # one edge: every arc
+    cnt = _check(g, od, 2, [(0, 1), (1, 0)])
+    assert cnt == h.info()[1]
+    # no match: 6-clique in a sparse graph
+    edges = [(a, b) for a in range(6) for b in range(6) if a != b]
+    assert g.count(cb.Query.from_arcs(6, edges)).count == 0
+    # empty data graph
+    e = cb.HostGraph.erdos_renyi(50, 0.0, seed=0).upload(0)
+    assert e.count(cb.Query.from_arcs(3, cb.named_query_arcs("triangle")[1])).count == 0
+
+
+def test_known_answers():
+    """Closed forms: K_n holds n!/(n-k)! embeddings of any k-vertex
+    connected symmetric query; a star K_{1,s} (s >= 2) in K_{1,d} has
+    d!/(d-s)! (the centre must map to the centre)."""
+    import math
+    n = 9
+    edges = [(a, b) for a in range(n) for b in range(n) if a != b]
+    src = np.array([a for a, _ in edges], np.uint32)
+    dst = np.array([b for _, b in edges], np.uint32)
+    oo, oa, io, ia, s, d = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo, oa)
+    for name in NAMED:
+        k, arcs = cb.named_query_arcs(name)
+        want = math.factorial(n) // math.factorial(n - k)
+        assert g.count(cb.Query.from_arcs(k, arcs)).count == want
+        assert g.count(cb.Query.from_arcs(k, arcs), flags=cb.FLAG_SYMMETRY_BREAK).count == want
+    dstar = 12
+    sedges = [(0, i) for i in range(1, dstar + 1)]
+    sarcs = sedges + [(b, a) for a, b in sedges]
+    s2 = np.array([a for a, _ in sarcs], np.uint32)
+    d2 = np.array([b for _, b in sarcs], np.uint32)
+    oo, oa, _, _, _, _ = csr_from_arcs(dstar + 1, s2, d2)
+    g = cb.Graph.from_csr(dstar + 1, oo, oa)
+    for s_ in (2, 3, 4):
+        qarcs = [(0, i) for i in range(1, s_ + 1)] + [(i, 0) for i in range(1, s_ + 1)]
+        want = math.factorial(dstar) // math.factorial(dstar - s_)
+        assert g.count(cb.Query.from_arcs(s_ + 1, qarcs)).count == want

@@ -1,0 +1,168 @@
+"""Host-side logic on CPU: the C-ABI library, loader semantics, generators,
+query plans, CLI argument handling.  No GPU compute is called."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import cuts_b200 as cb
+from oracle import oracle as O
+
+
+def test_library_exports_every_header_symbol():
+    with open(cb.HEADER_PATH) as f:
+        src = f.read()
+    declared = set(re.findall(r"\b(cuts_[a-z0-9_]+)\s*\(", src))
+    assert len(declared) >= 25
+    lib = cb.lib()
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    # and nothing exported beyond the header (plus C++ internals, hidden by the namespace)
+    out = subprocess.run(["nm", "-D", "--defined-only", cb.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    exported = set(re.findall(r" T (cuts_[a-z0-9_]+)$", out, re.M))
+    assert exported == declared
+
+
+def test_version():
+    assert cb.lib().cuts_version().decode().startswith("cuts_b200")
+
+
+CASES = {
+    "plain": "4\n0\t1\n1\t2\n2\t3\n3\t0\n",
+    "crlf": "4\r\n0\t1\r\n1\t2\r\n2\t3\r\n",
+    "no_tab_lines_skipped": "5\n# comment\n0\t1\n\n1 2\n3\t4\n",
+    "duplicates": "3\n0\t1\n0\t1\n1\t2\n0\t1\n",
+    "self_loops": "3\n0\t0\n0\t1\n2\t2\n",
+    "stoi_prefix": "6\t junk\n 1\t2xyz\n+3\t 4\n5\t0\t9\n",
+    "no_trailing_newline": "3\n0\t1\n1\t2",
+    "isolated": "10\n0\t9\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_loader_matches_oracle(tmp_path, name):
+    p = str(tmp_path / "g.txt")
+    with open(p, "w", newline="") as f:
+        f.write(CASES[name])
+    og = O.Graph.load(p)
+    h = cb.HostGraph.load(p)
+    n, arcs, sym, _ = h.info()
+    assert n == og.n
+    oo, oa, io, ia = og.csr()
+    po, pa, pi, pia = h.csr()
+    assert np.array_equal(oo, po) and np.array_equal(oa, pa)
+    assert sym == og.symmetric()
+    if not sym:
+        assert np.array_equal(io, pi) and np.array_equal(ia, pia)
+
+
+@pytest.mark.parametrize("text,code", [
+    ("", cb.ERR_PARSE),
+    ("x\n0\t1\n", cb.ERR_PARSE),
+    ("3\n0\t5\n", cb.ERR_PARSE),
+    ("3\n-1\t2\n", cb.ERR_PARSE),
+    ("3\n0\tx\n", cb.ERR_PARSE),
+    ("3\n99999999999\t1\n", cb.ERR_PARSE),
+])
+def test_loader_errors(tmp_path, text, code):
+    p = str(tmp_path / "bad.txt")
+    with open(p, "w") as f:
+        f.write(text)
+    with pytest.raises(cb.CutsError) as e:
+        cb.HostGraph.load(p)
+    assert e.value.code == code
+
+
+def test_missing_file():
+    with pytest.raises(cb.CutsError) as e:
+        cb.HostGraph.load("/nonexistent/graph.txt")
+    assert e.value.code == cb.ERR_IO
+
+
+def test_write_roundtrip(tmp_path):
+    h = cb.HostGraph.erdos_renyi(3000, 0.003, seed=7)
+    p = str(tmp_path / "er.txt")
+    h.write(p)
+    h2 = cb.HostGraph.load(p)
+    a, b = h.csr(), h2.csr()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_er_generator():
+    h = cb.HostGraph.erdos_renyi(10000, 8.0 / 9999, seed=0)
+    n, arcs, sym, _ = h.info()
+    assert n == 10000 and sym
+    assert abs(arcs / n - 8.0) < 0.3
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(n), np.diff(oo.astype(np.int64)))
+    assert not np.any(src == oa)  # no loops
+    h2 = cb.HostGraph.erdos_renyi(10000, 8.0 / 9999, seed=0)
+    assert np.array_equal(h2.csr()[1], oa)
+    h3 = cb.HostGraph.erdos_renyi(10000, 8.0 / 9999, seed=1)
+    assert not np.array_equal(h3.csr()[1][:1000], oa[:1000])
+
+
+def test_chung_lu_generator():
+    n, m = 20000, 100000
+    h = cb.HostGraph.chung_lu(n, m, 2.1, 2.0, 500.0, seed=0)
+    nn, arcs, sym, maxd = h.info()
+    assert nn == n and sym and arcs == 2 * m
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(n), np.diff(oo.astype(np.int64)))
+    assert not np.any(src == oa)
+    deg = np.diff(oo.astype(np.int64))
+    assert maxd == deg.max() and maxd > 20 * deg.mean()  # heavy tail
+    h2 = cb.HostGraph.chung_lu(n, m, 2.1, 2.0, 500.0, seed=0)
+    assert np.array_equal(h2.csr()[1], oa)
+
+
+def test_random_query_connected():
+    for seed in range(50):
+        k = 3 + seed % 6
+        arcs = cb.random_query_arcs(k, 0.3, seed)
+        q = cb.Query.from_arcs(k, arcs)  # raises when disconnected
+        assert sorted(q.order) == list(range(k))
+        assert all((b, a) in arcs for a, b in arcs)
+
+
+def test_query_errors():
+    with pytest.raises(cb.CutsError) as e:
+        cb.Query.from_arcs(4, [(0, 1), (1, 0), (2, 3), (3, 2)])
+    assert e.value.code == cb.ERR_QUERY
+    with pytest.raises(cb.CutsError) as e:
+        cb.Query.from_edges(17, [(i, i + 1) for i in range(16)])
+    assert e.value.code == cb.ERR_QUERY
+    q = cb.Query.from_edges(4, [(0, 1), (1, 2), (2, 3)])
+    with pytest.raises(cb.CutsError):
+        q.set_order([0, 2, 1, 3])  # position 1 has no arc to position 0
+    q.set_order([1, 2, 0, 3])
+    assert q.order == [1, 2, 0, 3]
+
+
+@pytest.mark.parametrize("name,aut", [("triangle", 6), ("4-cycle", 8), ("5-cycle", 10),
+                                      ("6-cycle", 12), ("house", 2), ("4-clique+pendant", 6),
+                                      ("3-prism", 12)])
+def test_automorphism_counts(name, aut):
+    k, arcs = cb.named_query_arcs(name)
+    assert cb.Query.from_arcs(k, arcs).automorphisms() == aut
+
+
+def test_automorphisms_directed():
+    # directed 3-cycle: rotations only
+    assert cb.Query.from_arcs(3, [(0, 1), (1, 2), (2, 0)]).automorphisms() == 3
+    # directed path: identity only
+    assert cb.Query.from_arcs(3, [(0, 1), (1, 2)]).automorphisms() == 1
+
+
+def test_cli_usage_and_bad_trunks(tmp_path):
+    r = subprocess.run([cb.CLI_PATH], capture_output=True, text=True)
+    assert r.returncode == 255
+    assert "args data_graph path,query_graph_path" in r.stdout
+    r = subprocess.run([cb.CLI_PATH, "a", "b", "0"], capture_output=True, text=True)
+    assert r.returncode == 255 and "invalid trunks" in r.stdout
+    r = subprocess.run([cb.CLI_PATH, "/nonexistent/d.txt", "/nonexistent/q.g"],
+                       capture_output=True, text=True)
+    assert r.returncode == 255 and "failed" in r.stdout
