@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark: exact subgraph-isomorphism counting on one B200.
+
+Workload (the mid-size plain-method configuration): an undirected Chung-Lu
+graph with n = 1,000,000 vertices and exactly 10,000,000 distinct edges
+(expected degrees from a power law with exponent 2.1, minimum 2, capped at
+20,000; seed 0), int32 CSR resident in HBM; queries triangle, 5-cycle, house
+(5 vertices, 6 edges) and 4-clique + pendant, each counted exactly along the
+score.cpp order with the root level cut into 4 chunks, as the reference's
+`cuts <data> <query> 4`.  The input is synthetic (this project's seeded
+generator): the reference's SNAP graphs are not used.
+
+One step = the four counts.  value = matches per second of device time
+(sum of counts / sum of device times; each count timed by CUDA events on the
+engine's stream from its first kernel to its last, as the reference times
+its search).  L2 is flushed (a 512 MB write) before every count, outside the
+timed intervals.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuts|reference]
+
+With N > 1 (torchrun, one rank per GPU) the roots are striped over ranks
+(u % N == rank, as the reference's multi-node level 0) and the four counts are
+summed over ranks; the total work is fixed, so scaling is "strong".
+
+--impl reference times the CPU oracle (a C/OpenMP restatement of the
+reference's algorithm, the same join order) on this host's cores over a
+bounded root sample of the same workload; the reference itself has no CPU
+implementation of the search.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "workload": "chung-lu n=1e6 m=1e7 gamma=2.1 cap=2e4; triangle,5-cycle,house,4-clique+pendant; chunks=4",
+    "n": 1_000_000, "m": 10_000_000, "gamma": 2.1, "wmin": 2.0, "cap": 20000.0, "seed": 0,
+    "queries": ["triangle", "5-cycle", "house", "4-clique+pendant"],
+    "chunks": 4,
+}
+METRIC = "matches/s (exact counts, 1M-vertex power-law graph, 4 queries)"
+UNIT = "matches/s"
+
+
+def _env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class Clocks:
+    """nvidia-smi samples of one GPU during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def make_graph():
+    import cuts_b200 as cb
+    w = WORKLOAD
+    return cb.HostGraph.chung_lu(w["n"], w["m"], w["gamma"], w["wmin"], w["cap"], w["seed"])
+
+
+def make_queries():
+    import cuts_b200 as cb
+    return [(name,) + cb.named_query_arcs(name) for name in WORKLOAD["queries"]]
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (cpu_baseline and --impl reference)
+# ---------------------------------------------------------------------------
+
+def cpu_sample(h, queries, budget_s=20.0):
+    """Time the oracle on a root sample of each query, sized so the whole sample
+    takes about budget_s seconds; returns (matches/s, cores, description)."""
+    from oracle import oracle as O
+    import numpy as np
+    oo, oa, _, _ = h.csr()
+    od = O.Graph.from_csr(h.n, oo, oa)
+    cores = os.cpu_count() or 1
+    total_cnt, total_t, parts = 0, 0.0, []
+    per_q = budget_s / len(queries)
+    for name, k, arcs in queries:
+        import cuts_b200 as cb
+        order = cb.Query.from_arcs(k, arcs).order
+        oq = O.Graph.from_arcs(k, arcs)
+        n0 = O.count(od, O.Graph.from_arcs(1, []))[1][0] if False else h.n
+        # grow a contiguous root slice (vertex-id order; weights are i.i.d. per
+        # vertex, so a slice is an unbiased sample) until it takes per_q / 4
+        span = 64
+        while True:
+            t0 = time.perf_counter()
+            cnt, lv, _ = O.count(od, oq, order, 0, span, cores)
+            dt = time.perf_counter() - t0
+            if dt >= per_q / 4 or span >= n0:
+                break
+            span = min(n0, span * 4 if dt < per_q / 64 else span * 2)
+        total_cnt += cnt
+        total_t += dt
+        parts.append(f"{name}: first {span} roots ({100.0 * span / n0:.3f}% of L_0) {dt:.2f}s")
+    return total_cnt / max(total_t, 1e-9), cores, "; ".join(parts)
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return 0
+    h = make_graph()
+    queries = make_queries()
+    for _ in range(args.warmup):
+        cpu_sample(h, queries, budget_s=args.cpu_budget / 2)
+    vals, desc, cores = [], "", 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, cores, desc = cpu_sample(h, queries, budget_s=args.cpu_budget / 2)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded Chung-Lu generator)",
+        "config": {"workload": WORKLOAD["workload"], "sample": "root slices per query"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# engine
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuts", choices=["cuts", "reference"])
+    ap.add_argument("--flags", type=int, default=0, help="CUTS_FLAG_* bits")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import cuts_b200 as cb
+
+    rank, world, local = _env_rank()
+    dev = local
+    torch.cuda.set_device(dev)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    h = make_graph()
+    n, arcs, sym, maxd = h.info()
+    g = h.upload(dev)
+    queries = [(name, cb.Query.from_arcs(k, a)) for name, k, a in make_queries()]
+    chunks = WORKLOAD["chunks"]
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
+
+    def count(q):
+        if world > 1:
+            return g.count_sharded(q, rank, world, chunks=chunks, flags=args.flags)
+        return g.count(q, chunks=chunks, flags=args.flags, stats=True)
+
+    def step(record):
+        ms, cnts, launches = 0.0, [], 0
+        for name, q in queries:
+            flush.fill_(len(cnts))
+            torch.cuda.synchronize(dev)
+            r = count(q)
+            ms += r.ms
+            cnts.append(r.count)
+            launches += r.launches
+            if record is not None:
+                record.append((name, r.count, r.ms))
+        return ms, cnts, launches
+
+    for _ in range(args.warmup):
+        step(None)
+
+    clocks = Clocks(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t0 = time.perf_counter()
+    total_ms, launches, per_query = 0.0, 0, []
+    counts = None
+    for _ in range(args.steps):
+        ms, cnts, la = step(per_query)
+        total_ms += ms
+        launches += la
+        counts = cnts
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+
+    counts_t = torch.tensor(counts, dtype=torch.float64)
+    ms_t = torch.tensor([total_ms], dtype=torch.float64)
+    if pg:
+        c64 = torch.tensor(counts, dtype=torch.int64, device=f"cuda:{dev}")
+        pg.all_reduce(c64)
+        counts = [int(x) for x in c64.cpu()]
+        mt = ms_t.to(f"cuda:{dev}")
+        pg.all_reduce(mt, op=pg.ReduceOp.MAX)
+        ms_t = mt.cpu()
+    step_matches = sum(counts)
+    max_ms = float(ms_t[0])
+    value = step_matches * args.steps / (max_ms / 1e3)
+
+    result = None
+    if rank == 0:
+        # live per-kernel timing for the roofline: one profiled pass (event
+        # pairs around every level launch) plus the traffic model
+        kern = {"last_level": [0.0, 0, 0], "expand": [0.0, 0, 0]}
+        if world == 1:
+            for name, q in queries:
+                flush.fill_(7)
+                torch.cuda.synchronize(dev)
+                r = g.count(q, chunks=chunks, flags=args.flags, stats=True, profile=True,
+                            alg_bytes=True)
+                kern["last_level"][0] += r.last_level_ms
+                kern["last_level"][1] += r.last_level_launches
+                kern["last_level"][2] += r.last_level_bytes
+                kern["expand"][0] += r.expand_ms
+                kern["expand"][1] += r.expand_launches
+        peak, peak_kind = measured_peaks()
+        ll_ms, ll_n, ll_bytes = kern["last_level"]
+        achieved = (ll_bytes / max(ll_n, 1)) / ((ll_ms / max(ll_n, 1)) / 1e3) / 1e9 if ll_ms else None
+        traffic = ncu_traffic().get("last_level_bytes_per_launch")
+        roofline = {
+            "kernel": "k_level<count> (last trie level)",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "peak_source": peak_kind,
+            "alg_bytes_per_launch": ll_bytes / max(ll_n, 1) if ll_n else None,
+            "avg_launch_ms": ll_ms / max(ll_n, 1) if ll_n else None,
+            "share_of_kernel_time": ll_ms / max(ll_ms + kern["expand"][0], 1e-12) if ll_ms else None,
+        }
+
+        # end to end through the C ABI: host CSR (pinned) -> device, counts, D2H of counts
+        oo, oa, _, _ = h.csr()
+        oo_p = torch.from_numpy(oo.view(np.int64)).pin_memory().numpy().view(np.uint64)
+        oa_p = torch.from_numpy(oa.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        h2d = oo_p.nbytes + oa_p.nbytes
+        e2e_t = []
+        for it in range(max(1, min(args.steps, 3)) + 1):
+            torch.cuda.synchronize(dev)
+            t1 = time.perf_counter()
+            g2 = cb.Graph.from_csr(n, oo_p, oa_p, device=dev)
+            tot = 0
+            for name, q in queries:
+                tot += g2.count(q, chunks=chunks, flags=args.flags).count
+            g2.close()
+            torch.cuda.synchronize(dev)
+            if it > 0:  # first pass warms the allocator
+                e2e_t.append(time.perf_counter() - t1)
+            assert tot == step_matches or world > 1
+        e2e_val = step_matches / statistics.median(e2e_t)
+
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, cores, desc = cpu_sample(h, [(nm,) + cb.named_query_arcs(nm) for nm, _ in queries],
+                                        budget_s=args.cpu_budget)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Chung-Lu generator; SNAP graphs not used)",
+            "config": {"workload": WORKLOAD["workload"], "n": n, "arcs": arcs, "max_degree": maxd,
+                       "flags": args.flags, "l2": "flushed (512 MB write) before every count",
+                       "parallelism": f"root stripes x{world}" if world > 1 else "1 GPU"},
+            "counts": dict(zip([nm for nm, _ in queries], counts)),
+            "ms_per_query": {nm: statistics.mean([t for a, c, t in per_query if a == nm])
+                             for nm, _ in queries} if world == 1 else None,
+            "wall_s_timed": wall,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": 8 * len(queries),
+                    "note": "wall clock: CSR upload + padded layout + 4 counts + count reads"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(result), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

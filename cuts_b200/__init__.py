@@ -27,7 +27,8 @@ CLI_PATH = os.path.join(_HERE, "bin", "cuts")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "cuts_b200.h")
 
 OK = 0
-ERR_ARG, ERR_IO, ERR_PARSE, ERR_CUDA, ERR_NOMEM, ERR_QUERY, ERR_CAPACITY, ERR_LIMIT = range(1, 9)
+ERR_ARG, ERR_IO, ERR_PARSE, ERR_CUDA, ERR_NOMEM, ERR_QUERY, ERR_CAPACITY, ERR_LIMIT, ERR_BUDGET = \
+    range(1, 10)
 MAX_QUERY = 16
 FLAG_SYMMETRY_BREAK = 1
 FLAG_NO_CLOSED_FORM = 2
@@ -45,7 +46,9 @@ _lib: Optional[C.CDLL] = None
 
 _u32p = C.POINTER(C.c_uint32)
 _u64p = C.POINTER(C.c_uint64)
+_fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
+FEATURES = 16
 
 _SIGS = {
     "cuts_last_error": (C.c_char_p, []),
@@ -75,11 +78,31 @@ _SIGS = {
     "cuts_count": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float)]),
     "cuts_count_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float),
                                 _u64p, _u64p]),
+    "cuts_count_sharded": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     _u64p, C.POINTER(C.c_float), _u64p]),
     "cuts_dump": (C.c_int, [_vp, _vp, C.c_char_p, _u64p]),
     "cuts_search": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, _u64p,
                               C.POINTER(C.c_float)]),
     "cuts_count_batch": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.c_uint32, _u64p,
                                    C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "cuts_count_budget": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_double, _u64p,
+                                    C.POINTER(C.c_float), _u64p]),
+    "cuts_batch_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.c_uint32, _u32p,
+                                    C.POINTER(_vp)]),
+    "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "cuts_batch_info": (C.c_int, [_vp, _u64p, _u32p]),
+    "cuts_batch_free": (None, [_vp]),
+    "cuts_mlp_create": (C.c_int, [C.c_uint32, C.c_uint64, C.c_int, C.POINTER(_vp)]),
+    "cuts_mlp_param_count": (C.c_int, [_vp, _u32p]),
+    "cuts_mlp_get_params": (C.c_int, [_vp, _fp]),
+    "cuts_mlp_set_params": (C.c_int, [_vp, _fp]),
+    "cuts_mlp_loss_grad": (C.c_int, [_vp, _fp, _fp, C.c_uint32, _fp, _fp]),
+    "cuts_mlp_train": (C.c_int, [_vp, _fp, _fp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, _fp]),
+    "cuts_mlp_predict": (C.c_int, [_vp, _fp, C.c_uint32, _fp]),
+    "cuts_mlp_free": (None, [_vp]),
+    "cuts_query_features": (C.c_int, [_vp, _vp, _u32p, _u64p, _fp]),
+    "cuts_plan": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_uint32, C.c_double, _u32p,
+                            C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 
@@ -239,6 +262,26 @@ class Query:
         Cl = [[int(x) for x in c[co[i]:co[i + 1]]] for i in range(k)]
         return P, Cl
 
+    def features(self, graph: "Graph", order: Sequence[int], level_sizes: Sequence[int]) -> np.ndarray:
+        """k x FEATURES rows of `order`, parent-level feature from level_sizes."""
+        k = self.k
+        o = np.array(order, np.uint32)
+        lv = np.array(level_sizes, np.uint64)
+        out = np.zeros((k, FEATURES), np.float32)
+        _check(lib().cuts_query_features(self._h, graph._h, _ptr(o, _u32p), _ptr(lv, _u64p),
+                                         _ptr(out, _fp)))
+        return out
+
+    def plan(self, graph: "Graph", mode: int = ORDER_SCORE, model: "Mlp" = None, beam: int = 0,
+             margin: float = 1.25):
+        """Choose and set the order; returns (order, predicted work, score-order work)."""
+        k = self.k
+        o = np.zeros(k, np.uint32)
+        pw, sw = C.c_double(), C.c_double()
+        _check(lib().cuts_plan(self._h, graph._h, mode, model._h if model else None, beam, margin,
+                               _ptr(o, _u32p), C.byref(pw), C.byref(sw)))
+        return [int(x) for x in o], pw.value, sw.value
+
     def automorphisms(self) -> int:
         a = C.c_uint64()
         _check(lib().cuts_query_automorphisms(self._h, C.byref(a)))
@@ -268,6 +311,10 @@ class CountResult:
     launches: int = 0
     chunks: int = 0
     last_level_bytes: int = 0
+    last_level_ms: float = 0.0
+    expand_ms: float = 0.0
+    last_level_launches: int = 0
+    expand_launches: int = 0
 
 
 class Graph:
@@ -305,19 +352,39 @@ class Graph:
         _check(lib().cuts_graph_set_level_cap(self._h, entries))
 
     def count(self, q: Query, chunks: int = 1, flags: int = 0, stats: bool = False,
-              alg_bytes: bool = False) -> CountResult:
+              alg_bytes: bool = False, profile: bool = False) -> CountResult:
         cnt, ms = C.c_uint64(), C.c_float()
-        if not stats and not alg_bytes:
+        if not stats and not alg_bytes and not profile:
             _check(lib().cuts_count(self._h, q._h, chunks, flags, C.byref(cnt), C.byref(ms)))
             return CountResult(cnt.value, ms.value)
         k = q.k
         lv = np.zeros(k, np.uint64)
-        st = np.zeros(3, np.uint64)
+        st = np.zeros(8, np.uint64)
         st[2] = 1 if alg_bytes else 0
+        st[3] = 1 if profile else 0
         _check(lib().cuts_count_ex(self._h, q._h, chunks, flags, C.byref(cnt), C.byref(ms),
                                    _ptr(lv, _u64p), _ptr(st, _u64p)))
         return CountResult(cnt.value, ms.value, [int(x) for x in lv], int(st[0]), int(st[1]),
-                           int(st[2]))
+                           int(st[2]), st[3] / 1e6, st[4] / 1e6, int(st[5]), int(st[6]))
+
+    def count_sharded(self, q: Query, shard: int, nshards: int, chunks: int = 1,
+                      flags: int = 0) -> CountResult:
+        cnt, ms = C.c_uint64(), C.c_float()
+        lv = np.zeros(q.k, np.uint64)
+        _check(lib().cuts_count_sharded(self._h, q._h, chunks, flags, shard, nshards,
+                                        C.byref(cnt), C.byref(ms), _ptr(lv, _u64p)))
+        return CountResult(cnt.value, ms.value, [int(x) for x in lv])
+
+    def count_budget(self, q: Query, budget_ms: float, chunks: int = 1, flags: int = 0):
+        """(CountResult, finished): stops between chunks once budget_ms has passed."""
+        cnt, ms = C.c_uint64(), C.c_float()
+        lv = np.zeros(q.k, np.uint64)
+        rc = lib().cuts_count_budget(self._h, q._h, chunks, flags, budget_ms, C.byref(cnt),
+                                     C.byref(ms), _ptr(lv, _u64p))
+        if rc == ERR_BUDGET:
+            return CountResult(0, budget_ms, [int(x) for x in lv]), False
+        _check(rc)
+        return CountResult(cnt.value, ms.value, [int(x) for x in lv]), True
 
     def dump(self, q: Query, path: str) -> int:
         n = C.c_uint64()
@@ -327,16 +394,128 @@ class Graph:
     def count_batch(self, queries: Sequence[Query], flags: int = 0):
         nq = len(queries)
         arr = (_vp * nq)(*[q._h for q in queries])
-        counts = np.zeros(nq, np.uint64)
-        status = (C.c_int * nq)()
+        counts = np.zeros(max(nq, 1), np.uint64)
+        status = (C.c_int * max(nq, 1))()
         ms = C.c_float()
         _check(lib().cuts_count_batch(self._h, arr, nq, flags, _ptr(counts, _u64p), status,
                                       C.byref(ms)))
-        return [int(x) for x in counts], list(status), ms.value
+        return [int(x) for x in counts[:nq]], list(status)[:nq], ms.value
+
+    def batch(self, queries: Sequence[Query], flags: int = 0, grain: int = 0,
+              tasks_per_grab: int = 0, blocks_per_sm: int = 0) -> "Batch":
+        return Batch(self, queries, flags, (grain, tasks_per_grab, blocks_per_sm))
 
     def close(self):
         if self._h:
             lib().cuts_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mlp:
+    """FP32 MLP cost model (in -> 64 -> 64 -> 1) resident on one GPU."""
+
+    def __init__(self, in_dim: int = FEATURES, seed: int = 0, device: int = 0):
+        h = _vp()
+        _check(lib().cuts_mlp_create(in_dim, seed, device, C.byref(h)))
+        self._h = h
+        self.in_dim = in_dim
+
+    @property
+    def n_params(self) -> int:
+        n = C.c_uint32()
+        _check(lib().cuts_mlp_param_count(self._h, C.byref(n)))
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        _check(lib().cuts_mlp_get_params(self._h, _ptr(p, _fp)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        _check(lib().cuts_mlp_set_params(self._h, _ptr(p, _fp)))
+
+    def loss_grad(self, X: np.ndarray, y: np.ndarray):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = C.c_float()
+        g = np.zeros(self.n_params, np.float32)
+        _check(lib().cuts_mlp_loss_grad(self._h, _ptr(X, _fp), _ptr(y, _fp), len(y), C.byref(loss),
+                                        _ptr(g, _fp)))
+        return loss.value, g
+
+    def train(self, X: np.ndarray, y: np.ndarray, epochs: int, batch: int = 0,
+              lr: float = 1e-3) -> float:
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = C.c_float()
+        _check(lib().cuts_mlp_train(self._h, _ptr(X, _fp), _ptr(y, _fp), len(y), epochs, batch, lr,
+                                    C.byref(loss)))
+        return loss.value
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        _check(lib().cuts_mlp_predict(self._h, _ptr(X, _fp), X.shape[0], _ptr(y, _fp)))
+        return y
+
+    def save(self, path: str) -> None:
+        np.save(path, self.get_params())
+
+    def load(self, path: str) -> None:
+        self.set_params(np.load(path))
+
+    def close(self):
+        if self._h:
+            lib().cuts_mlp_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many queries against one resident graph in one persistent launch,
+    captured once in a CUDA graph and replayed by run()."""
+
+    def __init__(self, graph: Graph, queries: Sequence[Query], flags: int = 0,
+                 tune: Tuple[int, int, int] = (0, 0, 0)):
+        self.graph = graph
+        self.queries = list(queries)  # keep the handles alive
+        nq = len(self.queries)
+        arr = (_vp * max(nq, 1))(*[q._h for q in self.queries])
+        t = np.array(tune, np.uint32)
+        h = _vp()
+        _check(lib().cuts_batch_create(graph._h, arr, nq, flags, _ptr(t, _u32p), C.byref(h)))
+        self._h = h
+        self.nq = nq
+
+    def run(self, budget_ms: float = 0.0):
+        """(counts, status, device ms); status ERR_BUDGET marks unfinished queries."""
+        counts = np.zeros(max(self.nq, 1), np.uint64)
+        status = (C.c_int * max(self.nq, 1))()
+        ms = C.c_float()
+        _check(lib().cuts_batch_run(self._h, budget_ms, _ptr(counts, _u64p), status, C.byref(ms)))
+        return [int(x) for x in counts[:self.nq]], list(status)[:self.nq], ms.value
+
+    def info(self):
+        t, b = C.c_uint64(), C.c_uint32()
+        _check(lib().cuts_batch_info(self._h, C.byref(t), C.byref(b)))
+        return t.value, b.value
+
+    def close(self):
+        if self._h:
+            lib().cuts_batch_free(self._h)
             self._h = None
 
     def __del__(self):

@@ -1,0 +1,495 @@
+// batch.cu -- many queries against one resident graph in one persistent
+// launch, captured in a CUDA graph.
+//
+// Work is a flat space of tasks, query-major: a task is (query q, root u,
+// range r of u's level-1 candidate list).  Roots are the data vertices in
+// out-degree order, so every query's root level is a prefix of one sorted
+// array, and a per-graph prefix sum of ceil(len / grain) turns a task index
+// into (u, r) with two binary searches -- nothing per query is materialised.
+// Warps take tasks from one global counter (work stealing across all SMs)
+// and run the query's levels depth-first from the task's level-1 range,
+// with a 32-candidate frontier per level in shared memory: the trie is
+// walked, never stored, so a batch needs no trie arena.  Each level step is
+// the same warp-cooperative join as the level kernels: candidates from the
+// shortest joined list, one per lane, lower-bound membership in the other
+// lists, ballot/popc compaction.  Counts accumulate per warp and are added
+// to the query's counter when the warp moves on.  A device-clock budget
+// stops the launch cleanly: tasks not finished mark their query incomplete.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "batch.hpp"
+#include "device_util.cuh"
+
+namespace cuts {
+
+#define BCK(call)                                                                      \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return set_error(CUTS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+constexpr int kBW = 8;  // warps per block
+
+struct BWarp {  // per-warp depth-first state, shared memory
+    uint32_t m[kBatchMaxK];
+    uint32_t moff[kBatchMaxK], mdeg[kBatchMaxK], x[kBatchMaxK], xend[kBatchMaxK];
+    uint32_t nb[kBatchMaxK], bi[kBatchMaxK], tmin[kBatchMaxK], nj[kBatchMaxK];
+    uint32_t joff[kBatchMaxK][kBatchMaxJ], jdeg[kBatchMaxK][kBatchMaxJ];
+    uint32_t buf[kBatchMaxK][32];
+};
+
+struct Ctx {
+    DevView g;
+    const BQuery *Q;
+    BWarp *S;
+    int lane;
+};
+
+// Joined lists of level d for the current prefix; the shortest feeds the
+// candidates, restricted to the symmetry window.  Warp-uniform.
+__device__ void enter_level(const Ctx &c, uint32_t d) {
+    const BLevel &L = c.Q->lv[d];
+    const uint32_t nj = L.nj;
+    uint32_t my_deg = kFullMask, my_off = 0;
+    if (uint32_t(c.lane) < nj) {
+        const uint32_t u = c.S->m[L.jpos[c.lane]];
+        const uint2 inf = L.jdir[c.lane] ? c.g.in_info[u] : c.g.out_info[u];
+        my_off = inf.x;
+        my_deg = inf.y;
+        c.S->joff[d][c.lane] = my_off;
+        c.S->jdeg[d][c.lane] = my_deg;
+    }
+    uint32_t bd = my_deg, bl = uint32_t(c.lane);
+    #pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        const uint32_t od = __shfl_xor_sync(kFullMask, bd, s), ol = __shfl_xor_sync(kFullMask, bl, s);
+        if (od < bd || (od == bd && ol < bl)) { bd = od; bl = ol; }
+    }
+    const uint32_t moff = __shfl_sync(kFullMask, my_off, int(bl));
+    uint32_t lo = 0, hi = kFullMask;
+    for (uint32_t msk = L.gt_mask; msk; msk &= msk - 1) lo = max(lo, c.S->m[__ffs(msk) - 1] + 1);
+    for (uint32_t msk = L.lt_mask; msk; msk &= msk - 1) hi = min(hi, c.S->m[__ffs(msk) - 1]);
+    const uint32_t *lst = c.g.adj + moff;
+    const uint32_t s0 = (lo && nj) ? lbound(lst, bd, lo) : 0;
+    const uint32_t e0 = nj ? (hi != kFullMask ? lbound(lst, bd, hi) : bd) : 0;
+    __syncwarp();
+    if (c.lane == 0) {
+        c.S->moff[d] = moff;
+        c.S->mdeg[d] = nj ? bd : 0;
+        c.S->tmin[d] = bl;
+        c.S->nj[d] = nj;
+        c.S->x[d] = s0;
+        c.S->xend[d] = max(s0, e0);
+        c.S->nb[d] = 0;
+        c.S->bi[d] = 0;
+    }
+    __syncwarp();
+}
+
+// Lane test of candidate list element idx at level d.
+__device__ __forceinline__ bool test_candidate(const Ctx &c, uint32_t d, uint32_t idx, uint32_t &cand) {
+    const BLevel &L = c.Q->lv[d];
+    bool ok = idx < c.S->xend[d];
+    const uint32_t v = ok ? __ldg(c.g.adj + c.S->moff[d] + idx) : 0;
+    if (ok)
+        for (uint32_t j = 0; j < d; ++j)
+            if (v == c.S->m[j]) { ok = false; break; }
+    if (ok && L.check_sig) {
+        const uint2 o = c.g.out_info[v], i = c.g.in_info[v];
+        ok = i.y >= L.qin && o.y >= L.qout;
+    }
+    if (ok) {
+        const uint32_t nj = c.S->nj[d], tm = c.S->tmin[d];
+        for (uint32_t t = 0; t < nj; ++t) {
+            if (t == tm) continue;
+            if (!contains(c.g.adj + c.S->joff[d][t], c.S->jdeg[d][t], v)) { ok = false; break; }
+        }
+    }
+    cand = v;
+    return ok;
+}
+
+// Candidates of level d in [x, xend), counted (the last level).
+__device__ unsigned long long count_level(const Ctx &c, uint32_t d) {
+    const BLevel &L = c.Q->lv[d];
+    const uint32_t s0 = c.S->x[d], e0 = c.S->xend[d];
+    if (s0 >= e0) return 0;
+    if (L.closed_form && c.S->nj[d] == 1) {
+        // one list, no signature: the window minus the matched vertices in it
+        const uint32_t *lst = c.g.adj + c.S->moff[d];
+        const uint32_t mdeg = c.S->mdeg[d];
+        bool hit = false;
+        if (uint32_t(c.lane) < d) {
+            const uint32_t mj = c.S->m[c.lane];
+            const uint32_t p = lbound(lst, mdeg, mj);
+            hit = p >= s0 && p < e0 && p < mdeg && __ldg(lst + p) == mj;
+        }
+        return (e0 - s0) - __popc(__ballot_sync(kFullMask, hit));
+    }
+    unsigned long long n = 0;
+    for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
+        uint32_t v;
+        const bool ok = test_candidate(c, d, x0 + c.lane, v);
+        n += __popc(__ballot_sync(kFullMask, ok));
+    }
+    return n;
+}
+
+// Next up-to-32 candidates of level d into its frontier buffer.
+__device__ void refill(const Ctx &c, uint32_t d) {
+    uint32_t v;
+    const bool ok = test_candidate(c, d, c.S->x[d] + c.lane, v);
+    const unsigned m = __ballot_sync(kFullMask, ok);
+    if (ok) c.S->buf[d][__popc(m & ((1u << c.lane) - 1))] = v;
+    __syncwarp();
+    if (c.lane == 0) {
+        c.S->x[d] += 32;
+        c.S->nb[d] = __popc(m);
+        c.S->bi[d] = 0;
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kBW * 32)
+k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
+        const unsigned long long *__restrict__ qbase, const uint32_t *__restrict__ vsorted,
+        const unsigned long long *__restrict__ pref0, const unsigned long long *__restrict__ pref1,
+        const unsigned long long *__restrict__ pref2, uint32_t grain, uint32_t tgrab,
+        unsigned long long *__restrict__ task_ctr, uint32_t *__restrict__ stop,
+        unsigned long long *__restrict__ counts, uint32_t *__restrict__ aborted,
+        unsigned long long budget_ns) {
+    __shared__ BWarp ws[kBW];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Ctx c{g, nullptr, &ws[warp], lane};
+    const unsigned long long total = qbase[nq];
+    const unsigned long long deadline = budget_ns ? global_ns() + budget_ns : ~0ull;
+    uint32_t cur = kFullMask;
+    unsigned long long qcount = 0;
+    volatile uint32_t *vstop = stop;
+
+    while (true) {
+        unsigned long long t0 = 0;
+        if (lane == 0) t0 = *vstop ? total : atomicAdd(task_ctr, (unsigned long long)tgrab);
+        t0 = __shfl_sync(kFullMask, t0, 0);
+        if (t0 >= total) break;
+        const unsigned long long t1 = min(t0 + tgrab, total);
+        for (unsigned long long t = t0; t < t1; ++t) {
+            if (cur == kFullMask || t < qbase[cur] || t >= qbase[cur + 1]) {
+                if (cur != kFullMask && lane == 0 && qcount) atomicAdd(&counts[cur], qcount);
+                qcount = 0;
+                uint32_t lo = 0, hi = nq - 1;  // last q with qbase[q] <= t
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (qbase[mid] <= t) lo = mid; else hi = mid - 1;
+                }
+                cur = lo;
+                c.Q = qs + cur;
+            }
+            if (*vstop || global_ns() > deadline) {
+                if (lane == 0) { atomicOr(stop, 1u); aborted[cur] = 1; }
+                continue;
+            }
+            const BQuery &Q = *c.Q;
+            const unsigned long long local = t - qbase[cur];
+            const unsigned long long *pref = Q.type == 0 ? pref0 : (Q.type == 1 ? pref1 : pref2);
+            uint32_t lo = 0, hi = Q.root_cnt - 1;  // root: last j with pref[j] <= local
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (pref[mid] <= local) lo = mid; else hi = mid - 1;
+            }
+            const uint32_t u = vsorted[lo];
+            const uint32_t r = uint32_t(local - pref[lo]);
+            const uint2 uo = g.out_info[u], ui = g.in_info[u];
+            if (ui.y < Q.lv[0].qin || uo.y < Q.lv[0].qout) continue;  // level-0 signature
+            if (lane == 0) c.S->m[0] = u;
+            __syncwarp();
+            // level 1: joins all on position 0; the task fixes the list and range
+            enter_level(c, 1);
+            {
+                // the task space was cut on the type's list (out, in or the
+                // shorter): make that list the candidate source
+                const bool use_in = Q.type == 1 || (Q.type == 2 && ui.y < uo.y);
+                const uint2 L1 = use_in ? ui : uo;
+                uint32_t tm = 0;
+                for (uint32_t t2 = 0; t2 < Q.lv[1].nj; ++t2)
+                    if ((Q.lv[1].jdir[t2] != 0) == use_in) { tm = t2; break; }
+                const uint32_t *lst = g.adj + L1.x;
+                uint32_t lo1 = 0, hi1 = kFullMask;
+                if (Q.lv[1].gt_mask) lo1 = u + 1;
+                if (Q.lv[1].lt_mask) hi1 = u;
+                const uint32_t s0 = lo1 ? lbound(lst, L1.y, lo1) : 0;
+                const uint32_t e0 = hi1 != kFullMask ? lbound(lst, L1.y, hi1) : L1.y;
+                const uint32_t xs = max(s0, min(r * grain, L1.y));
+                const uint32_t xe = min(e0, min(r * grain + grain, L1.y));
+                __syncwarp();
+                if (lane == 0) {
+                    c.S->moff[1] = L1.x;
+                    c.S->mdeg[1] = L1.y;
+                    c.S->tmin[1] = tm;
+                    c.S->x[1] = xs;
+                    c.S->xend[1] = max(xs, xe);
+                }
+                __syncwarp();
+            }
+            if (Q.k == 2) {
+                qcount += count_level(c, 1);
+                continue;
+            }
+            // depth-first over levels 1..k-2, counting level k-1
+            uint32_t d = 1;
+            bool abandoned = false;
+            while (d >= 1) {
+                if (c.S->bi[d] < c.S->nb[d]) {
+                    const uint32_t v = c.S->buf[d][c.S->bi[d]];
+                    __syncwarp();
+                    if (lane == 0) {
+                        c.S->bi[d]++;
+                        c.S->m[d] = v;
+                    }
+                    __syncwarp();
+                    enter_level(c, d + 1);
+                    if (d + 2 == Q.k) qcount += count_level(c, d + 1);
+                    else ++d;
+                } else if (c.S->x[d] < c.S->xend[d]) {
+                    if (*vstop || global_ns() > deadline) { abandoned = true; break; }
+                    refill(c, d);
+                } else {
+                    --d;
+                }
+            }
+            if (abandoned && lane == 0) {
+                atomicOr(stop, 1u);
+                aborted[cur] = 1;
+            }
+        }
+    }
+    if (cur != kFullMask && lane == 0 && qcount) atomicAdd(&counts[cur], qcount);
+}
+
+}  // namespace
+
+// ---- host ---------------------------------------------------------------------
+
+int batch_prepare_graph(DeviceGraph &g, uint32_t grain) {
+    if (g.batch_vsorted && g.batch_grain == grain) return CUTS_OK;
+    const uint32_t n = g.n;
+    std::vector<uint32_t> vs(n);
+    std::iota(vs.begin(), vs.end(), 0u);
+    std::stable_sort(vs.begin(), vs.end(),
+                     [&](uint32_t a, uint32_t b) { return g.h_out_deg[a] > g.h_out_deg[b]; });
+    const int types = g.symmetric ? 1 : 3;
+    std::vector<unsigned long long> pref(size_t(types) * (n + 1), 0);
+    for (int t = 0; t < types; ++t) {
+        unsigned long long *p = pref.data() + size_t(t) * (n + 1);
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t v = vs[j];
+            const uint32_t len = t == 0 ? g.h_out_deg[v]
+                                        : (t == 1 ? g.h_in_deg[v] : std::min(g.h_out_deg[v], g.h_in_deg[v]));
+            p[j + 1] = p[j] + std::max<uint32_t>(1, (len + grain - 1) / grain);
+        }
+    }
+    cudaFree(g.batch_vsorted);
+    cudaFree(g.batch_pref);
+    g.batch_vsorted = nullptr;
+    g.batch_pref = nullptr;
+    BCK(cudaMalloc(&g.batch_vsorted, sizeof(uint32_t) * std::max<uint32_t>(n, 1)));
+    BCK(cudaMalloc(&g.batch_pref, sizeof(unsigned long long) * pref.size()));
+    BCK(cudaMemcpy(g.batch_vsorted, vs.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(g.batch_pref, pref.data(), sizeof(unsigned long long) * pref.size(), cudaMemcpyHostToDevice));
+    g.batch_grain = grain;
+    g.batch_pref_host.swap(pref);
+    return CUTS_OK;
+}
+
+void Batch::destroy() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(d_queries);
+    cudaFree(d_qbase);
+    cudaFree(d_counts);
+    cudaFree(d_aborted);
+    cudaFree(d_ctr);
+    cudaFreeHost(h_counts);
+    cudaFreeHost(h_aborted);
+    cudaFreeHost(h_ctr);
+    exec = nullptr;
+    graph = nullptr;
+    d_queries = nullptr;
+    d_qbase = nullptr;
+    d_counts = nullptr;
+    d_aborted = nullptr;
+    d_ctr = nullptr;
+    h_counts = nullptr;
+    h_aborted = nullptr;
+    h_ctr = nullptr;
+}
+
+int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_t flags_,
+                  const BatchTuning &tune_) {
+    g = &dg;
+    flags = flags_;
+    tune = tune_;
+    if (tune.grain == 0) tune.grain = 64;
+    if (tune.tasks_per_grab == 0) tune.tasks_per_grab = 1;
+    BCK(cudaSetDevice(g->device));
+    int rc = batch_prepare_graph(*g, tune.grain);
+    if (rc) return rc;
+    queries = qs;
+    nq = uint32_t(qs.size());
+    std::vector<BQuery> hq;
+    std::vector<unsigned long long> qbase(1, 0);
+    aut.assign(nq, 1);
+    eligible.assign(nq, 0);
+    const uint32_t n = g->n;
+    for (uint32_t i = 0; i < nq; ++i) {
+        const Query &q = *qs[i];
+        Plan plan;
+        rc = build_plan(q, g->symmetric, flags, plan);
+        if (rc) return rc;
+        aut[i] = plan.aut;
+        BQuery b;
+        std::memset(&b, 0, sizeof(b));
+        bool ok = q.k >= 2 && q.k <= uint32_t(kBatchMaxK) && n > 0;
+        for (uint32_t d = 0; ok && d < q.k; ++d) {
+            const LevelPlan &L = plan.lv[d];
+            if (L.nj > uint32_t(kBatchMaxJ)) { ok = false; break; }
+            BLevel &B = b.lv[d];
+            B.nj = L.nj;
+            B.qin = L.qin;
+            B.qout = L.qout;
+            B.check_sig = L.check_sig;
+            B.gt_mask = L.gt_mask;
+            B.lt_mask = L.lt_mask;
+            B.closed_form = L.closed_form;
+            for (uint32_t t = 0; t < L.nj; ++t) {
+                B.jpos[t] = L.jpos[t];
+                B.jdir[t] = L.jdir[t];
+            }
+        }
+        unsigned long long tasks = 0;
+        if (ok) {
+            b.k = q.k;
+            bool has_out = false, has_in = false;
+            for (uint32_t t = 0; t < plan.lv[1].nj; ++t) (plan.lv[1].jdir[t] ? has_in : has_out) = true;
+            b.type = g->symmetric ? 0 : (has_out && has_in ? 2 : (has_in ? 1 : 0));
+            const uint32_t qout0 = plan.lv[0].qout;
+            b.root_cnt = qout0 < g->stats.out_ge.size() ? uint32_t(g->stats.out_ge[qout0]) : 0;
+            if (b.root_cnt == 0) {
+                ok = false;  // no root passes: the count is 0 without a launch
+            } else {
+                tasks = g->batch_pref_host[size_t(b.type) * (n + 1) + b.root_cnt];
+                hq.push_back(b);
+                qbase.push_back(qbase.back() + tasks);
+                index.push_back(i);
+            }
+        }
+        eligible[i] = ok ? 1 : (q.k >= 2 && n > 0 && q.k <= uint32_t(kBatchMaxK) ? 2 : 0);
+    }
+    // eligible: 1 = in the launch, 2 = no root (count 0), 0 = counted by the level engine
+    nb = uint32_t(hq.size());
+    total_tasks = qbase.back();
+    BCK(cudaMalloc(&d_queries, sizeof(BQuery) * std::max<size_t>(hq.size(), 1)));
+    BCK(cudaMalloc(&d_qbase, sizeof(unsigned long long) * qbase.size()));
+    BCK(cudaMalloc(&d_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1)));
+    BCK(cudaMalloc(&d_aborted, sizeof(uint32_t) * std::max<uint32_t>(nb, 1)));
+    BCK(cudaMalloc(&d_ctr, sizeof(unsigned long long) * 2));
+    BCK(cudaMallocHost(&h_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1)));
+    BCK(cudaMallocHost(&h_aborted, sizeof(uint32_t) * std::max<uint32_t>(nb, 1)));
+    BCK(cudaMallocHost(&h_ctr, sizeof(unsigned long long) * 2));
+    if (nb) {
+        BCK(cudaMemcpy(d_queries, hq.data(), sizeof(BQuery) * nb, cudaMemcpyHostToDevice));
+    }
+    BCK(cudaMemcpy(d_qbase, qbase.data(), sizeof(unsigned long long) * qbase.size(), cudaMemcpyHostToDevice));
+    qbase_host.swap(qbase);
+    return CUTS_OK;
+}
+
+int Batch::capture(unsigned long long budget_ns) {
+    if (exec && budget_ns == captured_budget) return CUTS_OK;
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    int bps = 0;
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch, kBW * 32, 0));
+    int sms = 0;
+    BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    if (tune.blocks_per_sm) bps = std::min<int>(bps, int(tune.blocks_per_sm));
+    const unsigned long long maxb = (total_tasks + kBW - 1) / kBW;
+    const uint32_t blocks = uint32_t(std::max<unsigned long long>(1, std::min<unsigned long long>(
+        (unsigned long long)(std::max(1, bps) * sms), maxb)));
+    const unsigned long long *pref = g->batch_pref;
+    const size_t stride = size_t(g->n) + 1;
+    cudaStream_t s = g->stream;
+    BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1), s);
+    cudaMemsetAsync(d_aborted, 0, sizeof(uint32_t) * std::max<uint32_t>(nb, 1), s);
+    cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 2, s);
+    if (nb) {
+        k_batch<<<blocks, kBW * 32, 0, s>>>(
+            DevView{g->out_info, g->in_info, g->adj, g->n}, d_queries, nb, d_qbase, g->batch_vsorted,
+            pref, g->symmetric ? pref : pref + stride, g->symmetric ? pref : pref + 2 * stride, tune.grain,
+            tune.tasks_per_grab, d_ctr, reinterpret_cast<uint32_t *>(d_ctr + 1), d_counts, d_aborted,
+            budget_ns);
+    }
+    cudaMemcpyAsync(h_counts, d_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1),
+                    cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_aborted, d_aborted, sizeof(uint32_t) * std::max<uint32_t>(nb, 1), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * 2, cudaMemcpyDeviceToHost, s);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &gr);
+    if (ce != cudaSuccess) return set_error(CUTS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    graph = gr;
+    BCK(cudaGraphInstantiate(&exec, graph, 0));
+    captured_budget = budget_ns;
+    launch_blocks = blocks;
+    return CUTS_OK;
+}
+
+int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int> &status, float *ms) {
+    BCK(cudaSetDevice(g->device));
+    const unsigned long long budget_ns = budget_ms > 0 ? (unsigned long long)(budget_ms * 1e6) : 0ull;
+    int rc = capture(budget_ns);
+    if (rc) return rc;
+    counts.assign(nq, 0);
+    status.assign(nq, CUTS_OK);
+    BCK(cudaEventRecord(g->ev0, g->stream));
+    BCK(cudaGraphLaunch(exec, g->stream));
+    BCK(cudaEventRecord(g->ev1, g->stream));
+    BCK(cudaStreamSynchronize(g->stream));
+    float t = 0;
+    BCK(cudaEventElapsedTime(&t, g->ev0, g->ev1));
+    const unsigned long long stop_at = std::min<unsigned long long>(h_ctr[0], total_tasks);
+    const bool stopped = reinterpret_cast<uint32_t *>(h_ctr + 1)[0] != 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint32_t i = index[b];
+        counts[i] = uint64_t(h_counts[b]) * aut[i];
+        const bool unfinished = h_aborted[b] || (stopped && qbase_host[b + 1] > stop_at);
+        if (unfinished) status[i] = CUTS_ERR_BUDGET;
+    }
+    // queries outside the batched kernel's limits: the level engine, one by one
+    for (uint32_t i = 0; i < nq; ++i) {
+        if (eligible[i] != 0) continue;
+        CountResult r;
+        CountOptions opt;
+        opt.flags = flags;
+        rc = device_count(*g, *queries[i], opt, r);
+        if (rc) {
+            status[i] = rc;
+            continue;
+        }
+        counts[i] = r.count;
+        t += r.ms;
+    }
+    if (ms) *ms = t;
+    return CUTS_OK;
+}
+
+}  // namespace cuts

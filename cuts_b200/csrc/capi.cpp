@@ -5,10 +5,14 @@
 #include <cstring>
 #include <iostream>
 #include <memory>
+#include <cmath>
 #include <new>
 
+#include "batch.hpp"
 #include "engine.hpp"
 #include "host.hpp"
+#include "mlp.hpp"
+#include "order_search.hpp"
 
 struct cuts_graph_s {
     cuts::DeviceGraph *dev = nullptr;
@@ -18,6 +22,14 @@ struct cuts_query_s {
 };
 struct cuts_hgraph_s {
     cuts::HostGraph g;
+};
+struct cuts_batch_s {
+    cuts::Batch b;
+    ~cuts_batch_s() { b.destroy(); }
+};
+struct cuts_mlp_s {
+    cuts::Mlp m;
+    ~cuts_mlp_s() { m.destroy(); }
 };
 
 using namespace cuts;
@@ -254,13 +266,12 @@ void cuts_query_free(cuts_query q) { delete q; }
 
 // ---- counting -----------------------------------------------------------------
 
-int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
-                  float *ms, uint64_t *level_sizes, uint64_t *stats) {
+static int count_impl(cuts_graph g, cuts_query q, const CountOptions &opt, uint64_t *count,
+                      float *ms, uint64_t *level_sizes, uint64_t *stats) {
     if (!g || !g->dev || !q) return set_error(CUTS_ERR_ARG, "null handle");
     GUARD(([&]() {
         CountResult r;
-        const bool want_bytes = stats && stats[2] != 0;
-        int rc = device_count(*g->dev, q->q, chunks, flags, want_bytes, r);
+        int rc = device_count(*g->dev, q->q, opt, r);
         if (rc) return rc;
         if (count) *count = r.count;
         if (ms) *ms = r.ms;
@@ -269,14 +280,49 @@ int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, u
             stats[0] = r.launches;
             stats[1] = r.chunks;
             stats[2] = r.last_level_bytes;
+            stats[3] = uint64_t(r.last_level_ms * 1e6);
+            stats[4] = uint64_t(r.expand_ms * 1e6);
+            stats[5] = r.last_level_launches;
+            stats[6] = r.expand_launches;
+            stats[7] = 0;
         }
         return CUTS_OK;
     })());
 }
 
+int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
+                  float *ms, uint64_t *level_sizes, uint64_t *stats) {
+    CountOptions opt;
+    opt.chunks = chunks;
+    opt.flags = flags;
+    opt.want_bytes = stats && stats[2] != 0;
+    opt.profile = stats && stats[3] != 0;
+    return count_impl(g, q, opt, count, ms, level_sizes, stats);
+}
+
+int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                       uint32_t shard, uint32_t nshards, uint64_t *count, float *ms,
+                       uint64_t *level_sizes) {
+    CountOptions opt;
+    opt.chunks = chunks;
+    opt.flags = flags;
+    opt.shard = shard;
+    opt.nshards = nshards;
+    return count_impl(g, q, opt, count, ms, level_sizes, nullptr);
+}
+
 int cuts_count(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
                float *ms) {
     return cuts_count_ex(g, q, chunks, flags, count, ms, nullptr, nullptr);
+}
+
+int cuts_count_budget(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                      double budget_ms, uint64_t *count, float *ms, uint64_t *level_sizes) {
+    CountOptions opt;
+    opt.chunks = chunks;
+    opt.flags = flags;
+    opt.budget_ms = budget_ms;
+    return count_impl(g, q, opt, count, ms, level_sizes, nullptr);
 }
 
 int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count) {
@@ -310,7 +356,9 @@ int cuts_search(const char *query_file, const char *data_file, int write_to_disk
         std::cout << (trunks ? "finish copying graph to gpu..." : "end copying graph to gpu...")
                   << std::endl;
         CountResult r;
-        rc = device_count(*dg, q, trunks ? trunks : 1, 0, false, r);
+        CountOptions opt;
+        opt.chunks = trunks ? trunks : 1;
+        rc = device_count(*dg, q, opt, r);
         if (rc) return rc;
         std::cout << base_name(data_file) << "," << base_name(query_file) << "," << r.ms << "ms,"
                   << r.count << std::endl;
@@ -327,11 +375,155 @@ int cuts_search(const char *query_file, const char *data_file, int write_to_disk
     })());
 }
 
+// ---- learned order ------------------------------------------------------------
+
+int cuts_mlp_create(uint32_t in_dim, uint64_t seed, int device, cuts_mlp *out) {
+    if (!out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_mlp_s>();
+        int rc = h->m.create(int(in_dim), seed, device);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_mlp_param_count(cuts_mlp m, uint32_t *n) {
+    if (!m || !n) return set_error(CUTS_ERR_ARG, "null argument");
+    *n = uint32_t(mlp_param_count(m->m.in));
+    return CUTS_OK;
+}
+
+int cuts_mlp_get_params(cuts_mlp m, float *params) {
+    if (!m || !params) return set_error(CUTS_ERR_ARG, "null argument");
+    return m->m.get_params(params);
+}
+
+int cuts_mlp_set_params(cuts_mlp m, const float *params) {
+    if (!m || !params) return set_error(CUTS_ERR_ARG, "null argument");
+    return m->m.set_params(params);
+}
+
+int cuts_mlp_loss_grad(cuts_mlp m, const float *X, const float *y, uint32_t n, float *loss,
+                       float *grad) {
+    if (!m || !X || !y || n == 0) return set_error(CUTS_ERR_ARG, "bad argument");
+    GUARD(m->m.loss_grad(X, y, int(n), loss, grad));
+}
+
+int cuts_mlp_train(cuts_mlp m, const float *X, const float *y, uint32_t n, uint32_t epochs,
+                   uint32_t batch, float lr, float *final_loss) {
+    if (!m || !X || !y || n == 0) return set_error(CUTS_ERR_ARG, "bad argument");
+    GUARD(m->m.train(X, y, int(n), int(epochs), int(batch), lr, final_loss));
+}
+
+int cuts_mlp_predict(cuts_mlp m, const float *X, uint32_t n, float *y) {
+    if (!m || !X || !y) return set_error(CUTS_ERR_ARG, "null argument");
+    if (n == 0) return CUTS_OK;
+    GUARD(m->m.predict(X, int(n), y));
+}
+
+void cuts_mlp_free(cuts_mlp m) { delete m; }
+
+int cuts_query_features(cuts_query q, cuts_graph g, const uint32_t *order,
+                        const uint64_t *level_sizes, float *features) {
+    if (!q || !g || !g->dev || !order || !features) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        const Query &Q = q->q;
+        for (uint32_t i = 0; i < Q.k; ++i) {
+            const float parent = (i && level_sizes) ? float(std::log1p(double(level_sizes[i - 1]))) : 0.f;
+            step_features(Q, g->dev->stats, order, i, parent, features + size_t(i) * kFeatures);
+        }
+        return CUTS_OK;
+    })());
+}
+
+int cuts_plan(cuts_query q, cuts_graph g, int mode, cuts_mlp m, uint32_t beam, double margin,
+              uint32_t *order_out, double *pred_work, double *score_work) {
+    if (!q || !g || !g->dev) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        Query &Q = q->q;
+        std::vector<uint32_t> order;
+        double pw = 0, sw = 0;
+        if (mode == CUTS_ORDER_LEARNED && m) {
+            OrderSearchOptions opt;
+            opt.beam = beam;
+            opt.margin = margin > 0 ? margin : 1.25;
+            OrderChoice ch;
+            int rc = learned_order(Q, g->dev->stats, m->m, opt, ch);
+            if (rc) return rc;
+            order = ch.order;
+            pw = ch.used_learned ? ch.best_work : ch.score_work;
+            sw = ch.score_work;
+        } else if (mode == CUTS_ORDER_SCORE || mode == CUTS_ORDER_LEARNED) {
+            int rc = score_order(Q, order);  // fallback when no model is given
+            if (rc) return rc;
+        } else {
+            return set_error(CUTS_ERR_ARG, "unknown order mode");
+        }
+        int rc = set_order(Q, order);
+        if (rc) return rc;
+        if (order_out) std::copy(order.begin(), order.end(), order_out);
+        if (pred_work) *pred_work = pw;
+        if (score_work) *score_work = sw;
+        return CUTS_OK;
+    })());
+}
+
+int cuts_batch_create(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                      const uint32_t *tune, cuts_batch *out) {
+    if (!g || !g->dev || !out || (nq && !qs)) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        std::vector<const Query *> v;
+        for (uint32_t i = 0; i < nq; ++i) {
+            if (!qs[i]) return set_error(CUTS_ERR_ARG, "null query in batch");
+            v.push_back(&qs[i]->q);
+        }
+        BatchTuning t;
+        if (tune) {
+            if (tune[0]) t.grain = tune[0];
+            if (tune[1]) t.tasks_per_grab = tune[1];
+            t.blocks_per_sm = tune[2];
+        }
+        auto h = std::make_unique<cuts_batch_s>();
+        int rc = h->b.create(*g->dev, v, flags, t);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
+int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status, float *ms) {
+    if (!b) return set_error(CUTS_ERR_ARG, "null batch");
+    GUARD(([&]() {
+        std::vector<uint64_t> c;
+        std::vector<int> st;
+        int rc = b->b.run(budget_ms, c, st, ms);
+        if (rc) return rc;
+        if (counts) std::copy(c.begin(), c.end(), counts);
+        if (status) std::copy(st.begin(), st.end(), status);
+        return CUTS_OK;
+    })());
+}
+
+int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks) {
+    if (!b) return set_error(CUTS_ERR_ARG, "null batch");
+    if (tasks) *tasks = b->b.total_tasks;
+    if (blocks) *blocks = b->b.launch_blocks;
+    return CUTS_OK;
+}
+
+void cuts_batch_free(cuts_batch b) { delete b; }
+
 int cuts_count_batch(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
                      uint64_t *counts, int *status, float *ms) {
-    if (!g || !g->dev || (nq && (!qs || !counts))) return set_error(CUTS_ERR_ARG, "null argument");
-    (void)flags; (void)status; (void)ms;
-    return set_error(CUTS_ERR_ARG, "batched counting not built yet");
+    cuts_batch b = nullptr;
+    int rc = cuts_batch_create(g, qs, nq, flags, nullptr, &b);
+    if (rc) return rc;
+    rc = cuts_batch_run(b, 0, counts, status, ms);
+    cuts_batch_free(b);
+    return rc;
 }
 
 }  // extern "C"

@@ -23,11 +23,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <charconv>
+#include <chrono>
 #include <climits>
+#include <cstdio>
+#include <memory>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "device_util.cuh"
 #include "engine.hpp"
 
 namespace cuts {
@@ -46,16 +51,11 @@ constexpr int kWarps = 8;       // warps per block in the level kernels
 constexpr int kOutBuf = 128;    // per-warp staged output entries
 constexpr uint32_t kTile = 256; // planner tile (parents)
 
-struct DevView {
-    const uint2 *out_info;
-    const uint2 *in_info;
-    const uint32_t *adj;
-    uint32_t n;
-};
-
 // Plan + level pointers, resident in device memory for the run.
 struct RunParams {
     Plan plan;
+    uint32_t stored;   // levels kept in HBM: k-1 when counting, k when dumping
+    uint32_t pad_[3];
     uint32_t *vert[kMaxK];
     uint32_t *par[kMaxK];
     uint32_t *ub[kMaxK];
@@ -63,35 +63,14 @@ struct RunParams {
 
 enum Mode { kExpand = 0, kCountMode = 1, kBytesMode = 2 };
 
-__device__ __forceinline__ uint32_t lbound(const uint32_t *__restrict__ a, uint32_t len,
-                                           uint32_t x) {
-    uint32_t lo = 0;
-    while (len > 0) {
-        uint32_t half = len >> 1;
-        if (__ldg(a + lo + half) < x) { lo += half + 1; len -= half + 1; }
-        else len = half;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ bool contains(const uint32_t *__restrict__ a, uint32_t len, uint32_t x) {
-    uint32_t p = lbound(a, len, x);
-    return p < len && __ldg(a + p) == x;
-}
-
-__device__ __forceinline__ uint32_t warp_min(uint32_t v) {
-    #pragma unroll
-    for (int s = 16; s; s >>= 1) v = min(v, __shfl_xor_sync(kFull, v, s));
-    return v;
-}
-
 // ---- level 0: signature scan (device_funcs.cu:267-279) ---------------
-__global__ void k_roots(DevView g, const RunParams *__restrict__ rp, uint32_t *__restrict__ n0) {
+__global__ void k_roots(DevView g, const RunParams *__restrict__ rp, uint32_t shard, uint32_t nshards,
+                        uint32_t *__restrict__ n0) {
     const Plan &P = rp->plan;
     const uint32_t qin = P.lv[0].qin, qout = P.lv[0].qout;
     // L_0 entries carry the child bound for level 1, whose joins all use
-    // position 0 (only needed when level 1 is stored, i.e. k >= 3)
-    const bool need_ub = P.k >= 3;
+    // position 0 (only needed when level 1 is stored)
+    const bool need_ub = rp->stored >= 2;
     bool use_out = false, use_in = false;
     if (P.k >= 2)
         for (uint32_t t = 0; t < P.lv[1].nj; ++t) (P.lv[1].jdir[t] ? use_in : use_out) = true;
@@ -101,7 +80,7 @@ __global__ void k_roots(DevView g, const RunParams *__restrict__ rp, uint32_t *_
         const uint32_t u = base + threadIdx.x;
         bool ok = false;
         uint32_t ub = UINT_MAX;
-        if (u < g.n) {
+        if (u < g.n && u % nshards == shard) {  // rank striding, device_funcs.cu:273
             const uint2 o = g.out_info[u], i = g.in_info[u];
             ok = o.y >= qout && i.y >= qin;
             if (use_out) ub = min(ub, o.y);
@@ -132,7 +111,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
     __shared__ LevelPlan sL, sN;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
-    __shared__ uint32_t s_k, s_sym;
+    __shared__ uint32_t s_k, s_sym, s_stored;
     __shared__ uint32_t wm[kWarps][kMaxK];
     __shared__ uint32_t joff[kWarps][kMaxJ], jdeg[kWarps][kMaxJ];
     __shared__ uint32_t ob_v[MODE == kExpand ? kWarps : 1][kOutBuf];
@@ -152,7 +131,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
             s_vert[threadIdx.x] = rp->vert[threadIdx.x];
             s_par[threadIdx.x] = rp->par[threadIdx.x];
         }
-        if (threadIdx.x == 0) { s_k = rp->plan.k; s_sym = rp->plan.symmetric; }
+        if (threadIdx.x == 0) { s_k = rp->plan.k; s_sym = rp->plan.symmetric; s_stored = rp->stored; }
     }
     __syncthreads();
 
@@ -161,7 +140,8 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
     uint32_t *my_m = wm[warp];
     const uint32_t k = s_k;
     const bool sym = s_sym != 0;
-    const bool need_ub = MODE == kExpand && lvl + 2 < k;
+    // entries of L_lvl need a child bound when level lvl+1 is stored too
+    const bool need_ub = MODE == kExpand && lvl + 1 < s_stored;
     uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
     uint32_t *out_p = MODE == kExpand ? rp->par[lvl] : nullptr;
     uint32_t *out_u = MODE == kExpand ? rp->ub[lvl] : nullptr;
@@ -493,6 +473,13 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     g->symmetric = hg.symmetric;
     g->max_deg = hg.max_degree();
     g->adj_words = adj.size();
+    g->stats = degree_stats(hg);
+    g->h_out_deg.resize(n);
+    g->h_in_deg.resize(n);
+    for (uint32_t v = 0; v < n; ++v) {
+        g->h_out_deg[v] = hg.out_deg(v);
+        g->h_in_deg[v] = hg.in_deg(v);
+    }
     auto fail = [&](cudaError_t e, const char *what) {
         device_graph_free(g);
         return set_error(CUTS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -549,6 +536,8 @@ void device_graph_free(DeviceGraph *g) {
     cudaFree(g->d_plan);
     cudaFree(g->d_tiles);
     cudaFree(g->d_bounds);
+    cudaFree(g->batch_vsorted);
+    cudaFree(g->batch_pref);
     cudaFreeHost(g->h_u32);
     cudaFreeHost(g->h_u64);
     cudaFreeHost(g->h_plan);
@@ -573,6 +562,14 @@ struct Run {
     uint32_t grain;
     bool bytes_mode;
     CountResult &res;
+    bool dump = false;
+    bool profile = false;
+    double budget_ms = 0;
+    std::chrono::steady_clock::time_point t_start = std::chrono::steady_clock::now();
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    FILE *dump_file = nullptr;
+    const Query *query = nullptr;
+    uint64_t dumped = 0;
 
     int sync() {
         CK(cudaStreamSynchronize(g.stream));
@@ -636,6 +633,12 @@ struct Run {
         uint32_t blocks = std::min<uint32_t>(uint32_t(g_level_blocks[mode]),
                                              (warps_needed + kWarps - 1) / kWarps);
         blocks = std::max<uint32_t>(blocks, 1);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (profile) {
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            CK(cudaEventRecord(e0, g.stream));
+        }
         if (mode == kExpand)
             k_level<kExpand><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
                 g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, g.d_u64);
@@ -646,14 +649,31 @@ struct Run {
             k_level<kBytesMode><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
                 g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, g.d_u64 + 2);
         CK(cudaGetLastError());
+        if (profile) {
+            CK(cudaEventRecord(e1, g.stream));
+            marks.push_back({mode, {e0, e1}});
+        }
         res.launches++;
         return CUTS_OK;
+    }
+
+    // Sums the profiled launch times per kernel (after a sync).
+    void collect_profile() {
+        for (auto &m : marks) {
+            float t = 0;
+            cudaEventElapsedTime(&t, m.second.first, m.second.second);
+            if (m.first == kExpand) { res.expand_ms += t; res.expand_launches++; }
+            else { res.last_level_ms += t; res.last_level_launches++; }
+            cudaEventDestroy(m.second.first);
+            cudaEventDestroy(m.second.second);
+        }
+        marks.clear();
     }
 
     // Expands parents [pa, pb) of L_{lvl-1}, depth first by chunks.
     int expand(uint32_t lvl, uint32_t pa, uint32_t pb) {
         if (pb <= pa) return CUTS_OK;
-        if (lvl + 1 == k) {
+        if (lvl + 1 == k && !dump) {
             int rc = launch_level(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
             return rc;
         }
@@ -663,6 +683,10 @@ struct Run {
         for (size_t c = 0; c + 1 < cuts.size(); ++c) {
             const uint32_t a = cuts[c], b = cuts[c + 1];
             if (b <= a) continue;
+            if (budget_ms > 0 &&
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count() >
+                    budget_ms)
+                return set_error(CUTS_ERR_BUDGET, "time budget exhausted");
             rc = launch_level(kExpand, lvl, a, b);
             if (rc) return rc;
             res.chunks++;
@@ -676,28 +700,48 @@ struct Run {
             if (g.h_u32[kSlotErr] || nout > cap)
                 return set_error(CUTS_ERR_CAPACITY, "level " + std::to_string(lvl) + " overflowed its capacity");
             res.level_sizes[lvl] += nout;
-            rc = expand(lvl + 1, 0, nout);
+            rc = (dump && lvl + 1 == k) ? write_rows(nout) : expand(lvl + 1, 0, nout);
             if (rc) return rc;
         }
         return CUTS_OK;
     }
+
+    // Dump: materialise the nout complete matches of L_{k-1} in pieces and
+    // write one ans.txt line per match, pairs in matching order
+    // (util.cpp:53-74).
+    int write_rows(uint32_t nout);
 };
 
 }  // namespace
 
-int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags, bool want_bytes,
-                 CountResult &res) {
-    res = CountResult();
-    if (chunks == 0) return set_error(CUTS_ERR_ARG, "chunks must be >= 1");
-    CK(cudaSetDevice(g.device));
-    int rc = launch_geometry();
-    if (rc) return rc;
+namespace {
+
+// Rows of complete matches: row r = the path of L_{k-1} entry first + r,
+// k words in matching order.
+__global__ void k_materialize(const RunParams *__restrict__ rp, uint32_t first, uint32_t nrows,
+                              uint32_t *__restrict__ rows) {
+    const uint32_t k = rp->plan.k;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
+        uint32_t e = first + r;
+        uint32_t *row = rows + size_t(r) * k;
+        for (int lv = int(k) - 1; lv >= 0; --lv) {
+            row[lv] = rp->vert[lv][e];
+            if (lv > 0) e = rp->par[lv][e];
+        }
+    }
+}
+
+constexpr uint32_t kDumpRows = 1u << 22;  // rows materialised per piece
+
+// Carves the arena for `stored` levels and uploads the run parameters.
+int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, RunParams *&hp,
+            RunParams *&dp, uint64_t &cap) {
     const uint32_t k = q.k;
-    RunParams *hp = static_cast<RunParams *>(g.h_plan);
+    hp = static_cast<RunParams *>(g.h_plan);
     std::memset(hp, 0, sizeof(RunParams));
-    rc = build_plan(q, g.symmetric, flags, hp->plan);
+    int rc = build_plan(q, g.symmetric, flags, hp->plan);
     if (rc) return rc;
-    // arena: L_0 (vert, ub) with n entries, then L_1..L_{k-2} (vert, par, ub)
+    hp->stored = stored;
     if (!g.arena) {
         cudaError_t e = cudaMalloc(&g.arena, g.arena_bytes);
         if (e != cudaSuccess) {
@@ -705,17 +749,17 @@ int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags
             return set_error(CUTS_ERR_NOMEM, "arena allocation failed: " + std::string(cudaGetErrorString(e)));
         }
     }
+    // L_0: vert + ub (n entries each); L_1..L_{stored-1}: vert + par + ub
     const uint64_t n = g.n;
     const uint64_t l0_bytes = ((8 * n + 255) / 256) * 256 + 256;
-    uint64_t cap = 0;
+    cap = 0;
     if (g.arena_bytes < l0_bytes) return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level");
-    if (k >= 3) {
-        if (g.arena_bytes <= l0_bytes) return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level");
-        cap = (g.arena_bytes - l0_bytes) / (12ull * (k - 2));
+    if (stored >= 2) {
+        cap = (g.arena_bytes - l0_bytes) / (12ull * (stored - 1));
         cap = std::min<uint64_t>(cap, (1ull << 31) - 64);
         if (g.level_cap_req) cap = std::min<uint64_t>(cap, g.level_cap_req);
         cap &= ~uint64_t(63);
-        if (cap < 2ull * std::max<uint32_t>(g.max_deg, 1) || cap == 0)
+        if (cap < 2ull * std::max<uint32_t>(g.max_deg, 1))
             return set_error(CUTS_ERR_CAPACITY, "level capacity below twice the maximum degree");
     }
     char *base = static_cast<char *>(g.arena);
@@ -723,62 +767,134 @@ int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags
     hp->ub[0] = reinterpret_cast<uint32_t *>(base + ((4 * n + 255) / 256) * 256);
     hp->par[0] = nullptr;
     char *cur = base + l0_bytes;
-    for (uint32_t i = 1; i + 1 < k; ++i) {
+    for (uint32_t i = 1; i < stored; ++i) {
         hp->vert[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
         hp->par[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
         hp->ub[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
     }
-    RunParams *dp = static_cast<RunParams *>(g.d_plan);
+    dp = static_cast<RunParams *>(g.d_plan);
     CK(cudaMemcpyAsync(dp, hp, sizeof(RunParams), cudaMemcpyHostToDevice, g.stream));
+    return CUTS_OK;
+}
 
-    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
-    CK(cudaEventRecord(g.ev0, g.stream));
+// Level 0 into L_0; returns |L_0|.
+int run_roots(DeviceGraph &g, Run &run, uint32_t shard, uint32_t nshards, uint32_t &n0) {
     CK(cudaMemsetAsync(g.d_u32, 0, sizeof(uint32_t) * kSlots, g.stream));
     CK(cudaMemsetAsync(g.d_u64, 0, sizeof(unsigned long long) * 8, g.stream));
-    uint32_t n0 = 0;
-    if (g.n) {
-        const uint32_t threads = 256;
-        const uint32_t blocks = std::min<uint32_t>((g.n + threads - 1) / threads, uint32_t(g_num_sms) * 8);
-        k_roots<<<blocks, threads, 0, g.stream>>>(run.view, dp, g.d_u32 + kSlotN0);
-        CK(cudaGetLastError());
-        res.launches++;
-        CK(cudaMemcpyAsync(g.h_u32 + kSlotN0, g.d_u32 + kSlotN0, sizeof(uint32_t), cudaMemcpyDeviceToHost, g.stream));
-        rc = run.sync();
+    n0 = 0;
+    if (!g.n) return CUTS_OK;
+    const uint32_t threads = 256;
+    const uint32_t blocks = std::min<uint32_t>((g.n + threads - 1) / threads, uint32_t(g_num_sms) * 8);
+    k_roots<<<blocks, threads, 0, g.stream>>>(run.view, run.dp, shard, nshards, g.d_u32 + kSlotN0);
+    CK(cudaGetLastError());
+    run.res.launches++;
+    CK(cudaMemcpyAsync(g.h_u32 + kSlotN0, g.d_u32 + kSlotN0, sizeof(uint32_t), cudaMemcpyDeviceToHost, g.stream));
+    int rc = run.sync();
+    if (rc) return rc;
+    n0 = g.h_u32[kSlotN0];
+    return CUTS_OK;
+}
+
+// Root slices, as the reference's trunks (host_funcs.cu:66-72).
+int run_slices(Run &run, uint32_t n0, uint32_t chunks) {
+    const uint32_t slice = uint32_t((uint64_t(n0) - 1) / chunks + 1);
+    for (uint32_t s = 0; s < chunks; ++s) {
+        const uint64_t a = uint64_t(s) * slice;
+        if (a >= n0) break;
+        int rc = run.expand(1, uint32_t(a), uint32_t(std::min<uint64_t>(a + slice, n0)));
         if (rc) return rc;
-        n0 = g.h_u32[kSlotN0];
     }
+    return CUTS_OK;
+}
+
+}  // namespace
+
+int Run::write_rows(uint32_t nout) {
+    const uint32_t k = this->k;
+    const std::vector<uint32_t> &order = query->order;
+    uint32_t *d_rows = nullptr, *h_rows = nullptr;
+    const uint32_t piece = std::min<uint32_t>(nout, kDumpRows);
+    CK(cudaMalloc(&d_rows, sizeof(uint32_t) * size_t(piece) * k));
+    cudaError_t e = cudaMallocHost(&h_rows, sizeof(uint32_t) * size_t(piece) * k);
+    if (e != cudaSuccess) {
+        cudaFree(d_rows);
+        return set_error(CUTS_ERR_NOMEM, "pinned dump buffer");
+    }
+    std::vector<char> text;
+    int rc = CUTS_OK;
+    for (uint32_t first = 0; first < nout && rc == CUTS_OK; first += piece) {
+        const uint32_t nr = std::min(piece, nout - first);
+        k_materialize<<<std::max<uint32_t>(1, std::min<uint32_t>((nr + 255) / 256, 4096)), 256, 0, g.stream>>>(
+            dp, first, nr, d_rows);
+        res.launches++;
+        if ((e = cudaMemcpyAsync(h_rows, d_rows, sizeof(uint32_t) * size_t(nr) * k, cudaMemcpyDeviceToHost,
+                                 g.stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(g.stream)) != cudaSuccess) {
+            rc = set_error(CUTS_ERR_CUDA, std::string("dump copy: ") + cudaGetErrorString(e));
+            break;
+        }
+        text.resize(size_t(nr) * k * 24 + 16);
+        char *w = text.data(), *end = text.data() + text.size();
+        for (uint32_t r = 0; r < nr; ++r) {
+            const uint32_t *row = h_rows + size_t(r) * k;
+            for (uint32_t j = 0; j < k; ++j) {
+                *w++ = '(';
+                w = std::to_chars(w, end, order[j]).ptr;
+                *w++ = ',';
+                w = std::to_chars(w, end, row[j]).ptr;
+                *w++ = ')';
+            }
+            *w++ = '\n';
+        }
+        if (std::fwrite(text.data(), 1, size_t(w - text.data()), dump_file) != size_t(w - text.data()))
+            rc = set_error(CUTS_ERR_IO, "short write to the dump file");
+        dumped += nr;
+    }
+    cudaFree(d_rows);
+    cudaFreeHost(h_rows);
+    return rc;
+}
+
+int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountResult &res) {
+    res = CountResult();
+    if (opt.chunks == 0) return set_error(CUTS_ERR_ARG, "chunks must be >= 1");
+    if (opt.nshards == 0 || opt.shard >= opt.nshards) return set_error(CUTS_ERR_ARG, "bad shard");
+    CK(cudaSetDevice(g.device));
+    int rc = launch_geometry();
+    if (rc) return rc;
+    const uint32_t k = q.k;
+    RunParams *hp = nullptr, *dp = nullptr;
+    uint64_t cap = 0;
+    rc = prepare(g, q, opt.flags, k - 1, hp, dp, cap);
+    if (rc) return rc;
+    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
+    run.profile = opt.profile;
+    run.budget_ms = opt.budget_ms;
+    CK(cudaEventRecord(g.ev0, g.stream));
+    uint32_t n0 = 0;
+    rc = run_roots(g, run, opt.shard, opt.nshards, n0);
+    if (rc) return rc;
     res.level_sizes[0] = n0;
     if (k >= 2 && n0 > 0) {
-        // root slices, as the reference's trunks (host_funcs.cu:66-72)
-        const uint32_t slice = uint32_t((uint64_t(n0) - 1) / chunks + 1);
-        for (uint32_t s = 0; s < chunks; ++s) {
-            const uint64_t a = uint64_t(s) * slice;
-            if (a >= n0) break;
-            const uint32_t b = uint32_t(std::min<uint64_t>(a + slice, n0));
-            rc = run.expand(1, uint32_t(a), b);
-            if (rc) return rc;
-        }
+        rc = run_slices(run, n0, opt.chunks);
+        if (rc) return rc;
     }
     CK(cudaEventRecord(g.ev1, g.stream));
     CK(cudaMemcpyAsync(g.h_u64, g.d_u64, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
     rc = run.sync();
     if (rc) return rc;
+    run.collect_profile();
     CK(cudaEventElapsedTime(&res.ms, g.ev0, g.ev1));
     const uint64_t raw = k >= 2 ? uint64_t(g.h_u64[0]) : 0;
     res.level_sizes[k - 1] = k >= 2 ? raw : n0;
     res.count = raw * hp->plan.aut;
-    if (want_bytes && k >= 2 && n0 > 0) {
+    if (opt.want_bytes && k >= 2 && n0 > 0) {
         // untimed second pass: algorithmic bytes of the last-level kernel
         CountResult tmp;
         Run r2{g, run.view, hp, dp, k, cap, 4, true, tmp};
         CK(cudaMemsetAsync(g.d_u64 + 2, 0, sizeof(unsigned long long), g.stream));
-        const uint32_t slice = uint32_t((uint64_t(n0) - 1) / chunks + 1);
-        for (uint32_t s = 0; s < chunks; ++s) {
-            const uint64_t a = uint64_t(s) * slice;
-            if (a >= n0) break;
-            rc = r2.expand(1, uint32_t(a), uint32_t(std::min<uint64_t>(a + slice, n0)));
-            if (rc) return rc;
-        }
+        rc = run_slices(r2, n0, opt.chunks);
+        if (rc) return rc;
         CK(cudaMemcpyAsync(g.h_u64 + 2, g.d_u64 + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
         rc = r2.sync();
         if (rc) return rc;
@@ -787,8 +903,34 @@ int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags
     return CUTS_OK;
 }
 
-int device_dump(DeviceGraph &, const Query &, const char *, uint64_t *) {
-    return set_error(CUTS_ERR_ARG, "dump not built yet");
+int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines) {
+    CK(cudaSetDevice(g.device));
+    int rc = launch_geometry();
+    if (rc) return rc;
+    const uint32_t k = q.k;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return set_error(CUTS_ERR_IO, std::string("cannot write ") + path);
+    std::unique_ptr<FILE, int (*)(FILE *)> hold(f, std::fclose);
+    if (lines) *lines = 0;
+    if (k < 2) return CUTS_OK;  // the reference dumps nothing for a 1-vertex query
+    RunParams *hp = nullptr, *dp = nullptr;
+    uint64_t cap = 0;
+    rc = prepare(g, q, CUTS_FLAG_NO_CLOSED_FORM, k, hp, dp, cap);
+    if (rc) return rc;
+    CountResult res;
+    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
+    run.dump = true;
+    run.dump_file = f;
+    run.query = &q;
+    uint32_t n0 = 0;
+    rc = run_roots(g, run, 0, 1, n0);
+    if (rc) return rc;
+    if (n0 > 0) {
+        rc = run_slices(run, n0, 1);
+        if (rc) return rc;
+    }
+    if (lines) *lines = run.dumped;
+    return CUTS_OK;
 }
 
 }  // namespace cuts

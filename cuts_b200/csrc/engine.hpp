@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "host.hpp"
+#include "order_search.hpp"
 
 namespace cuts {
 
@@ -39,6 +40,14 @@ struct DeviceGraph {
     void *h_plan = nullptr;                // pinned
     uint32_t *h_bounds = nullptr;          // pinned
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DegreeStats stats;                     // degree tails, for order features
+    std::vector<uint32_t> h_out_deg, h_in_deg;
+
+    // batched engine: vertices in out-degree order and task prefix sums
+    uint32_t *batch_vsorted = nullptr;
+    unsigned long long *batch_pref = nullptr;
+    std::vector<unsigned long long> batch_pref_host;
+    uint32_t batch_grain = 0;
 };
 
 int device_graph_upload(const HostGraph &g, int device, DeviceGraph **out);
@@ -51,13 +60,26 @@ struct CountResult {
     uint64_t launches = 0;
     uint64_t chunks = 0;
     uint64_t last_level_bytes = 0;
+    // per-kernel device time when profiling (CUDA events around each launch)
+    double last_level_ms = 0, expand_ms = 0;
+    uint64_t last_level_launches = 0, expand_launches = 0;
+};
+
+// Run options beyond the query.
+struct CountOptions {
+    uint32_t chunks = 1;      // root slices (the reference's trunks)
+    uint32_t flags = 0;       // CUTS_FLAG_*
+    uint32_t shard = 0;       // roots u with u % nshards == shard
+    uint32_t nshards = 1;
+    bool want_bytes = false;  // untimed pass for the last-level traffic model
+    bool profile = false;     // event pairs around every level launch
+    double budget_ms = 0;     // > 0: stop launching chunks after this much time
 };
 
 // Counts embeddings of q (order already set) in g.  chunks >= 1 slices the
 // root level like the reference's trunks.  want_bytes adds an untimed pass
 // computing the last-level kernel's algorithmic traffic.
-int device_count(DeviceGraph &g, const Query &q, uint32_t chunks, uint32_t flags,
-                 bool want_bytes, CountResult &res);
+int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountResult &res);
 
 // Enumerates every embedding and writes ans.txt lines (util.cpp:53-74).
 int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines);

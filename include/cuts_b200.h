@@ -25,6 +25,7 @@ extern "C" {
 #define CUTS_ERR_QUERY 6      /* query unsupported (disconnected, too large) */
 #define CUTS_ERR_CAPACITY 7   /* a level exceeds its capacity */
 #define CUTS_ERR_LIMIT 8      /* graph exceeds a size limit of the layout */
+#define CUTS_ERR_BUDGET 9     /* stopped by the caller's time budget */
 
 #define CUTS_MAX_QUERY 16     /* query vertices (reference: QUERY_NODES 12) */
 
@@ -145,12 +146,29 @@ int cuts_count(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
 
 /* As cuts_count, and also reports per-level sizes |L_0|..|L_{k-1}|
  * (level_sizes has k entries; with CUTS_FLAG_SYMMETRY_BREAK they are the
- * constrained sizes) and launch statistics: stats[0] = kernels launched,
- * stats[1] = chunks expanded, stats[2] = bytes of algorithmic traffic of
- * the last-level kernel (only when stats[2] is nonzero on entry: an extra
- * untimed pass computes it). */
+ * constrained sizes) and statistics in stats[8]:
+ *   [0] kernels launched, [1] chunks expanded,
+ *   [2] algorithmic bytes of the last-level kernel (computed by an extra
+ *       untimed pass, only when stats[2] is nonzero on entry),
+ *   [3] last-level kernel device time in ns, [4] expansion kernel time in
+ *       ns, [5] last-level launches, [6] expansion launches (event pairs
+ *       around every launch, only when stats[3] is nonzero on entry),
+ *   [7] reserved. */
 int cuts_count_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
                   uint64_t *count, float *ms, uint64_t *level_sizes, uint64_t *stats);
+
+/* Count only the roots u with u % nshards == shard, the rank striding of
+ * the reference's multi-node level 0 (device_funcs.cu:267-279,
+ * main_mpi.cu:257-376); the shard counts of 0..nshards-1 sum to the count,
+ * and so do the per-level sizes (level_sizes: k entries, may be NULL). */
+int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                       uint32_t shard, uint32_t nshards, uint64_t *count, float *ms,
+                       uint64_t *level_sizes);
+
+/* As cuts_count, but stops with CUTS_ERR_BUDGET once budget_ms of host time
+ * has passed (checked between chunks; the running chunk completes). */
+int cuts_count_budget(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                      double budget_ms, uint64_t *count, float *ms, uint64_t *level_sizes);
 
 /* Write every embedding to `path` in the reference's ans.txt line format
  * "(q,d)(q,d)..." in matching order (util.cpp:53-74).  Returns the number
@@ -164,13 +182,65 @@ int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count);
 int cuts_search(const char *query_file, const char *data_file, int write_to_disk,
                 uint32_t trunks, uint64_t *count, float *ms);
 
+/* ---- learned matching order ---------------------------------------- */
+
+/* The cost model of the learned order: an FP32 MLP in -> 64 -> 64 -> 1
+ * (ReLU) predicting log(1 + |L_i|) from per-step order features, trained and
+ * evaluated by this library's own kernels.  No reference counterpart: the
+ * reference has only the greedy score order (graph.cpp:62-93). */
+#define CUTS_FEATURES 16
+typedef struct cuts_mlp_s *cuts_mlp;
+int cuts_mlp_create(uint32_t in_dim, uint64_t seed, int device, cuts_mlp *out);
+int cuts_mlp_param_count(cuts_mlp m, uint32_t *n);
+int cuts_mlp_get_params(cuts_mlp m, float *params);
+int cuts_mlp_set_params(cuts_mlp m, const float *params);
+/* Mean squared error over n rows and its gradient (n_params floats). */
+int cuts_mlp_loss_grad(cuts_mlp m, const float *X, const float *y, uint32_t n, float *loss,
+                       float *grad);
+/* Adam, `epochs` passes over mini-batches of `batch` rows (0 = full batch). */
+int cuts_mlp_train(cuts_mlp m, const float *X, const float *y, uint32_t n, uint32_t epochs,
+                   uint32_t batch, float lr, float *final_loss);
+int cuts_mlp_predict(cuts_mlp m, const float *X, uint32_t n, float *y);
+void cuts_mlp_free(cuts_mlp m);
+
+/* Feature rows (k x CUTS_FEATURES) of the given order on graph g, with the
+ * parent-level feature taken from level_sizes (teacher forcing). */
+int cuts_query_features(cuts_query q, cuts_graph g, const uint32_t *order,
+                        const uint64_t *level_sizes, float *features);
+
+/* Choose and set the query's order.  CUTS_ORDER_SCORE: the score order
+ * (graph.cpp:62-93).  CUTS_ORDER_LEARNED: search connected-prefix orders
+ * (exhaustive, or a beam of `beam` prefixes when beam > 0) with the model m
+ * and keep the best unless its predicted work is not `margin` times below
+ * the score order's, in which case the score order stays.  order_out (k),
+ * pred_work and score_work (predicted work of the chosen and of the score
+ * order) may be NULL. */
+int cuts_plan(cuts_query q, cuts_graph g, int mode, cuts_mlp m, uint32_t beam, double margin,
+              uint32_t *order_out, double *pred_work, double *score_work);
+
 /* ---- batched counting -------------------------------------------- */
 
 /* Count nq queries against one resident graph in one persistent launch.
  * counts[nq] receives exact per-query counts; status[nq] (may be NULL)
- * receives 0 or a CUTS_ERR_* code per query. */
+ * receives 0 or a CUTS_ERR_* code per query.  No reference counterpart
+ * (the reference runs one query per process). */
 int cuts_count_batch(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
                      uint64_t *counts, int *status, float *ms);
+
+/* A reusable batch: the launch is captured once in a CUDA graph and replayed
+ * by every cuts_batch_run.  tune[3] = {grain (level-1 candidates per task),
+ * tasks per work-counter grab, max blocks per SM}; NULL or 0 entries take
+ * the defaults.  The query handles must outlive the batch. */
+typedef struct cuts_batch_s *cuts_batch;
+int cuts_batch_create(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                      const uint32_t *tune, cuts_batch *out);
+/* budget_ms > 0 stops the launch after that much device time; unfinished
+ * queries get status CUTS_ERR_BUDGET and a partial count.  *ms is the
+ * device time of the launch. */
+int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status, float *ms);
+/* tasks in the launch, launch blocks */
+int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks);
+void cuts_batch_free(cuts_batch b);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,116 @@
+"""Batched engine on a GPU: per-query counts of one persistent launch (replayed
+from its CUDA graph) against the CPU oracle, plus the time-budget status."""
+import numpy as np
+import pytest
+
+import cuts_b200 as cb
+from oracle import oracle as O
+from tests.helpers import csr_from_arcs, directed_er, oracle_graph_from_host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pl():
+    h = cb.HostGraph.chung_lu(3000, 12000, 2.2, 2.0, 60.0, seed=8)
+    return h, h.upload(0), oracle_graph_from_host(h)
+
+
+def _queries(n, seed0):
+    out = []
+    for s in range(n):
+        k = 3 + (s * 7 + seed0) % 3
+        p = [0.3, 0.45, 0.6][s % 3]
+        out.append((k, cb.random_query_arcs(k, p, seed0 + s)))
+    return out
+
+
+_WANT = {}
+
+
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK])
+def test_batch_counts_match_oracle(pl, flags):
+    h, g, od = pl
+    qdefs = _queries(48, 500)
+    qs = [cb.Query.from_arcs(k, a) for k, a in qdefs]
+    if "pl48" not in _WANT:
+        _WANT["pl48"] = [O.count(od, O.Graph.from_arcs(k, a))[0] for k, a in qdefs]
+    want = _WANT["pl48"]
+    b = g.batch(qs, flags=flags)
+    for rep in range(2):  # second run replays the captured graph
+        counts, status, ms = b.run()
+        assert status == [0] * len(qs)
+        assert counts == want
+
+
+@pytest.mark.parametrize("grain,grab,bps", [(1, 1, 0), (7, 3, 1), (256, 8, 2)])
+def test_batch_tuning_does_not_change_counts(pl, grain, grab, bps):
+    h, g, od = pl
+    qdefs = _queries(16, 900)
+    qs = [cb.Query.from_arcs(k, a) for k, a in qdefs]
+    want = [g.count(q).count for q in qs]
+    counts, status, _ = g.batch(qs, grain=grain, tasks_per_grab=grab, blocks_per_sm=bps).run()
+    assert counts == want and status == [0] * len(qs)
+
+
+def test_batch_named_and_edge_cases(pl):
+    h, g, od = pl
+    names = ["triangle", "4-cycle", "5-cycle", "house", "4-clique+pendant", "3-prism", "6-cycle"]
+    qs = [cb.Query.from_arcs(*cb.named_query_arcs(nm)) for nm in names]
+    # an edge (k = 2), a 6-clique (no match at all), and an 11-vertex path (beyond
+    # the batched kernel's 10 vertices: counted by the level engine)
+    qs.append(cb.Query.from_arcs(2, [(0, 1), (1, 0)]))
+    clique = [(a, b) for a in range(6) for b in range(6) if a != b]
+    qs.append(cb.Query.from_arcs(6, clique))
+    path11 = [(i, i + 1) for i in range(10)] + [(i + 1, i) for i in range(10)]
+    qs.append(cb.Query.from_arcs(11, path11[:]))
+    want = [g.count(q).count for q in qs]
+    counts, status, _ = g.count_batch(qs)
+    assert counts == want and status == [0] * len(qs)
+    assert counts[-4] == h.info()[1]
+
+
+def test_batch_directed():
+    n, src, dst = directed_er(1200, 12.0, seed=13)
+    oo, oa, io, ia, s, d = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo, oa, io, ia)
+    od = O.Graph.from_arrays(n, s, d)
+    rng = np.random.default_rng(1)
+    qdefs = []
+    for t in range(20):
+        k = 3 + t % 4
+        und = cb.random_query_arcs(k, 0.5, 300 + t)
+        qdefs.append((k, [a for a in und if a[0] < a[1] or rng.random() < 0.6]))
+    qs = [cb.Query.from_arcs(k, a) for k, a in qdefs]
+    want = [O.count(od, O.Graph.from_arcs(k, a))[0] for k, a in qdefs]
+    counts, status, _ = g.count_batch(qs)
+    assert counts == want
+
+
+def test_batch_budget_marks_unfinished():
+    """A tiny device-time budget ends the launch; unfinished queries say so,
+    finished ones keep exact counts, and the graph stays usable."""
+    h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
+    g = h.upload(0)
+    qs = [cb.Query.from_arcs(*cb.named_query_arcs("5-cycle")) for _ in range(8)]
+    b = g.batch(qs)
+    counts, status, ms = b.run(budget_ms=0.05)
+    assert any(s == cb.ERR_BUDGET for s in status)
+    full, st2, _ = b.run()
+    assert st2 == [0] * len(qs) and len(set(full)) == 1
+    for c, s in zip(counts, status):
+        if s == 0:
+            assert c == full[0]
+    assert g.count(qs[0]).count == full[0]
+
+
+def test_level_engine_budget():
+    h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
+    g = h.upload(0)
+    g.set_level_cap(4096)  # many chunks, so the budget is checked often
+    q = cb.Query.from_arcs(*cb.named_query_arcs("house"))
+    r, done = g.count_budget(q, 0.001)
+    assert not done
+    g.set_level_cap(0)
+    r, done = g.count_budget(q, 0.0)
+    assert done and r.count == g.count(q).count

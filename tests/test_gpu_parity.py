@@ -24,14 +24,24 @@ def er2k():
 
 @pytest.fixture(scope="module")
 def cl5k():
-    h = cb.HostGraph.chung_lu(5000, 30000, 2.1, 2.0, 400.0, seed=5)
+    # power law, exponent 2.1, degree cap 100: 5-cycles ~3.5e7, 6-cycles ~1.1e9
+    h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
     return h, h.upload(0), oracle_graph_from_host(h)
+
+
+_ORACLE = {}
+
+
+def oracle_count(od, k, arcs, order):
+    key = (id(od), k, tuple(arcs), tuple(order))
+    if key not in _ORACLE:
+        _ORACLE[key] = O.count(od, O.Graph.from_arcs(k, arcs), order)
+    return _ORACLE[key]
 
 
 def _check(g, od, k, arcs, flags=0, chunks=1, levels=True):
     q = cb.Query.from_arcs(k, arcs)
-    oq = O.Graph.from_arcs(k, arcs)
-    cnt, lv, _ = O.count(od, oq, q.order)
+    cnt, lv, _ = oracle_count(od, k, arcs, q.order)
     r = g.count(q, chunks=chunks, flags=flags, stats=True)
     assert r.count == cnt
     if levels:
@@ -46,7 +56,10 @@ def test_named_er(er2k, name):
     _check(g, od, k, arcs)
 
 
-@pytest.mark.parametrize("name", ["triangle", "4-cycle", "house", "4-clique+pendant"])
+PL_NAMED = ["triangle", "4-cycle", "5-cycle", "house", "4-clique+pendant", "3-prism"]
+
+
+@pytest.mark.parametrize("name", PL_NAMED)
 def test_named_power_law(cl5k, name):
     h, g, od = cl5k
     k, arcs = cb.named_query_arcs(name)
@@ -84,13 +97,27 @@ def test_trunks(er2k, trunks):
     _check(g, od, k, arcs, chunks=trunks)
 
 
-@pytest.mark.parametrize("name", NAMED)
+@pytest.mark.parametrize("name", PL_NAMED)
 def test_symmetry_breaking(cl5k, name):
     h, g, od = cl5k
     k, arcs = cb.named_query_arcs(name)
     q = cb.Query.from_arcs(k, arcs)
-    cnt, _, _ = O.count(od, O.Graph.from_arcs(k, arcs), q.order)
+    cnt, _, _ = oracle_count(od, k, arcs, q.order)
     assert g.count(q, flags=cb.FLAG_SYMMETRY_BREAK).count == cnt
+
+
+def test_heavy_count_engines_agree(cl5k):
+    """6-cycles (~1e9 embeddings, beyond the oracle's seconds): the level
+    engine, the level engine with symmetry breaking, chunked, and the
+    depth-first batched engine are independent paths and must agree."""
+    h, g, od = cl5k
+    q = cb.Query.from_arcs(*cb.named_query_arcs("6-cycle"))
+    a = g.count(q).count
+    assert a > 10**8
+    assert g.count(q, flags=cb.FLAG_SYMMETRY_BREAK).count == a
+    assert g.count(q, chunks=5).count == a
+    counts, status, _ = g.count_batch([q, q])
+    assert counts == [a, a] and status == [0, 0]
 
 
 @pytest.mark.parametrize("name", ["triangle", "4-clique+pendant", "5-cycle"])
@@ -179,3 +206,15 @@ def test_known_answers():
         qarcs = [(0, i) for i in range(1, s_ + 1)] + [(i, 0) for i in range(1, s_ + 1)]
         want = math.factorial(dstar) // math.factorial(dstar - s_)
         assert g.count(cb.Query.from_arcs(s_ + 1, qarcs)).count == want
+
+
+@pytest.mark.parametrize("name", ["triangle", "house", "4-clique+pendant"])
+def test_sharded_counts_sum(cl5k, name):
+    """Root stripes u % N == r partition the count and every level."""
+    h, g, od = cl5k
+    k, arcs = cb.named_query_arcs(name)
+    q = cb.Query.from_arcs(k, arcs)
+    full = g.count(q, stats=True)
+    parts = [g.count_sharded(q, r, 3) for r in range(3)]
+    assert sum(p.count for p in parts) == full.count
+    assert [sum(p.level_sizes[i] for p in parts) for i in range(k)] == full.level_sizes
