@@ -151,11 +151,11 @@ def cpu_sample(h, queries, budget_s=20.0):
     cores = os.cpu_count() or 1
     total_cnt, total_t, parts = 0, 0.0, []
     per_q = budget_s / len(queries)
+    import cuts_b200 as cb
     for name, k, arcs in queries:
-        import cuts_b200 as cb
         order = cb.Query.from_arcs(k, arcs).order
         oq = O.Graph.from_arcs(k, arcs)
-        n0 = O.count(od, O.Graph.from_arcs(1, []))[1][0] if False else h.n
+        n0 = h.n
         # grow a contiguous root slice (vertex-id order; weights are i.i.d. per
         # vertex, so a slice is an unbiased sample) until it takes per_q / 4
         span = 64
@@ -278,17 +278,11 @@ def main():
         pg.barrier()
     clk = clocks.stop()
 
-    counts_t = torch.tensor(counts, dtype=torch.float64)
-    ms_t = torch.tensor([total_ms], dtype=torch.float64)
+    max_ms = total_ms
     if pg:
-        c64 = torch.tensor(counts, dtype=torch.int64, device=f"cuda:{dev}")
-        pg.all_reduce(c64)
-        counts = [int(x) for x in c64.cpu()]
-        mt = ms_t.to(f"cuda:{dev}")
-        pg.all_reduce(mt, op=pg.ReduceOp.MAX)
-        ms_t = mt.cpu()
+        from cuts_b200.dist import reduce_counts
+        counts, max_ms = reduce_counts(counts, total_ms, device=f"cuda:{dev}")
     step_matches = sum(counts)
-    max_ms = float(ms_t[0])
     value = step_matches * args.steps / (max_ms / 1e3)
 
     result = None

@@ -1,0 +1,78 @@
+"""Autotuner for the batched engine's launch shape.
+
+Tries each (grain, tasks per grab, blocks per SM) on a sample of the batch,
+replays each candidate's captured CUDA graph a few times, and keeps the
+fastest configuration whose counts agree with the first one tried (the count
+never depends on the shape; disagreement would be a bug and raises).
+Results can be stored per GPU model and graph in a small JSON file.
+"""
+from __future__ import annotations
+
+import json
+import os
+import statistics
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple
+
+import cuts_b200 as cb
+
+GRAINS = (16, 32, 64, 128, 256)
+GRABS = (1, 4)
+BLOCKS = (0, 4)
+
+
+def tune_batch(g: "cb.Graph", queries: Sequence["cb.Query"], flags: int = 0,
+               grains: Iterable[int] = GRAINS, grabs: Iterable[int] = GRABS,
+               blocks: Iterable[int] = BLOCKS, reps: int = 3, budget_ms: float = 0.0):
+    """Returns (best (grain, grab, blocks), {config: median ms})."""
+    times: Dict[Tuple[int, int, int], float] = {}
+    ref: Optional[List[int]] = None
+    for gr in grains:
+        for tg in grabs:
+            for bl in blocks:
+                b = g.batch(queries, flags=flags, grain=gr, tasks_per_grab=tg, blocks_per_sm=bl)
+                ms = []
+                for _ in range(reps):
+                    counts, status, t = b.run(budget_ms)
+                    if any(s != 0 for s in status):
+                        break
+                    if ref is None:
+                        ref = counts
+                    elif counts != ref:
+                        raise RuntimeError(f"batch counts depend on the launch shape {gr, tg, bl}")
+                    ms.append(t)
+                b.close()
+                if len(ms) == reps:
+                    times[(gr, tg, bl)] = statistics.median(ms)
+    if not times:
+        return (64, 1, 0), times
+    best = min(times, key=times.get)
+    return best, times
+
+
+def gpu_key(g: "cb.Graph") -> str:
+    n, arcs, sym, maxd = g.info()
+    try:
+        import torch
+        name = torch.cuda.get_device_name(0)
+    except Exception:
+        name = "gpu"
+    return f"{name}|n={n}|arcs={arcs}|maxd={maxd}"
+
+
+def load(path: str, key: str) -> Optional[Tuple[int, int, int]]:
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    v = d.get(key)
+    return tuple(v) if v else None
+
+
+def store(path: str, key: str, cfg: Tuple[int, int, int]) -> None:
+    d = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+    d[key] = list(cfg)
+    with open(path, "w") as f:
+        json.dump(d, f, indent=1)

@@ -192,6 +192,17 @@ int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries) {
     return CUTS_OK;
 }
 
+int cuts_graph_set_arena_bytes(cuts_graph g, uint64_t bytes) {
+    if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
+    DeviceGraph &d = *g->dev;
+    cudaSetDevice(d.device);
+    cudaStreamSynchronize(d.stream);
+    cudaFree(d.arena);
+    d.arena = nullptr;
+    d.arena_bytes = bytes ? size_t(bytes) : d.arena_default;
+    return CUTS_OK;
+}
+
 void cuts_graph_free(cuts_graph g) {
     if (!g) return;
     device_graph_free(g->dev);

@@ -26,6 +26,7 @@
 #include <charconv>
 #include <chrono>
 #include <climits>
+#include <cstdlib>
 #include <cstdio>
 #include <memory>
 #include <cstring>
@@ -316,6 +317,216 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
     }
 }
 
+// ---- levels 1..k-1, flattened form ------------------------------------
+// A warp takes 32 consecutive parents, one per lane.  Each lane rebuilds its
+// parent's partial match (32 pointer chases in flight at once), gathers its
+// joined lists and picks the shortest.  The candidate lists of the 32
+// parents are then treated as one concatenated sequence: an inclusive warp
+// scan of their lengths gives every lane, at every step, the parent that
+// owns candidate f = step*32 + lane (a 5-step binary search over the scan
+// with shuffles), so all 32 lanes stay busy whether the lists hold 2 or
+// 20,000 entries.  Per-parent state lives in the owner lane's registers
+// (read with shuffles) and in shared memory laid out [join][lane], so lanes
+// reading different owners hit different banks.  Last-level parents with a
+// single joined list and no signature are counted by the closed form, one
+// parent per lane.
+constexpr int kFW = 4;    // warps per block
+constexpr int kFJ = 16;   // joined lists per level in this form
+
+template <int MODE>
+__global__ void __launch_bounds__(kFW * 32)
+k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, uint32_t pb,
+             uint32_t *__restrict__ cursor, uint32_t *__restrict__ out_n, uint32_t out_cap,
+             uint32_t *__restrict__ err, unsigned long long *__restrict__ acc) {
+    __shared__ LevelPlan sL, sN;
+    __shared__ uint32_t *s_vert[kMaxK];
+    __shared__ uint32_t *s_par[kMaxK];
+    __shared__ uint32_t s_k, s_sym, s_stored;
+    __shared__ uint32_t sm_m[kFW][kMaxK][33];   // [position][lane]
+    __shared__ uint32_t sm_off[kFW][kFJ][32], sm_deg[kFW][kFJ][32];
+    __shared__ uint32_t ob_v[MODE == kExpand ? kFW : 1][kOutBuf];
+    __shared__ uint32_t ob_p[MODE == kExpand ? kFW : 1][kOutBuf];
+    __shared__ uint32_t ob_u[MODE == kExpand ? kFW : 1][kOutBuf];
+    {
+        const uint32_t words = sizeof(LevelPlan) / 4;
+        const uint32_t *srcL = reinterpret_cast<const uint32_t *>(&rp->plan.lv[lvl]);
+        uint32_t *dL = reinterpret_cast<uint32_t *>(&sL);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dL[i] = srcL[i];
+        const uint32_t nl = lvl + 1 < rp->plan.k ? lvl + 1 : lvl;
+        const uint32_t *srcN = reinterpret_cast<const uint32_t *>(&rp->plan.lv[nl]);
+        uint32_t *dN = reinterpret_cast<uint32_t *>(&sN);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dN[i] = srcN[i];
+        if (threadIdx.x < kMaxK) {
+            s_vert[threadIdx.x] = rp->vert[threadIdx.x];
+            s_par[threadIdx.x] = rp->par[threadIdx.x];
+        }
+        if (threadIdx.x == 0) { s_k = rp->plan.k; s_sym = rp->plan.symmetric; s_stored = rp->stored; }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lanemask_lt = (1u << lane) - 1;
+    const bool sym = s_sym != 0;
+    const bool need_ub = MODE == kExpand && lvl + 1 < s_stored;
+    uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
+    uint32_t *out_p = MODE == kExpand ? rp->par[lvl] : nullptr;
+    uint32_t *out_u = MODE == kExpand ? rp->ub[lvl] : nullptr;
+    bool ub_out = false, ub_in = false;
+    if (need_ub)
+        for (uint32_t t = 0; t < sN.nj; ++t)
+            if (sN.jpos[t] == lvl) (sN.jdir[t] ? ub_in : ub_out) = true;
+    const uint32_t nj = sL.nj;
+    const bool check_sig = sL.check_sig != 0;
+    const bool load_info = check_sig || ub_out || ub_in;
+    const bool closed = MODE == kCountMode && sL.closed_form;
+    const uint32_t total = pb - pa;
+    unsigned long long local = 0;
+    uint32_t obn = 0;
+
+    auto flush = [&]() {
+        if constexpr (MODE != kExpand) return;
+        __syncwarp();
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(out_n, obn);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base + obn <= out_cap && base + obn >= base) {
+            for (uint32_t i = lane; i < obn; i += 32) {
+                out_v[base + i] = ob_v[warp][i];
+                out_p[base + i] = ob_p[warp][i];
+                if (need_ub) out_u[base + i] = ob_u[warp][i];
+            }
+        } else if (lane == 0) {
+            atomicOr(err, 1u);
+        }
+        obn = 0;
+        __syncwarp();
+    };
+
+    while (true) {
+        uint32_t start = 0;
+        if (lane == 0) start = atomicAdd(cursor, 32u);
+        start = __shfl_sync(kFullMask, start, 0);
+        if (start >= total) break;
+        const uint32_t p = pa + start + lane;
+        const bool have = start + lane < total;
+        // this lane's parent: partial match into column `lane`
+        if (have) {
+            uint32_t e = p;
+            for (int j = int(lvl) - 1; j >= 0; --j) {
+                sm_m[warp][j][lane] = s_vert[j][e];
+                if (j > 0) e = s_par[j][e];
+            }
+        }
+        // joined lists, shortest first
+        uint32_t moff = 0, mdeg = 0, tmin = 0, s0 = 0, e0 = 0, ubp = kFullMask;
+        unsigned long long bytes = 0;
+        if (have) {
+            mdeg = kFullMask;
+            for (uint32_t t = 0; t < nj; ++t) {
+                const uint32_t u = sm_m[warp][sL.jpos[t]][lane];
+                const uint2 inf = sL.jdir[t] ? g.in_info[u] : g.out_info[u];
+                sm_off[warp][t][lane] = inf.x;
+                sm_deg[warp][t][lane] = inf.y;
+                if (MODE == kBytesMode) bytes += 4ull * inf.y + 8;
+                if (inf.y < mdeg) { mdeg = inf.y; moff = inf.x; tmin = t; }
+            }
+            if (nj == 0) mdeg = 0;
+            uint32_t lo = 0, hi = kFullMask;
+            for (uint32_t msk = sL.gt_mask; msk; msk &= msk - 1) lo = max(lo, sm_m[warp][__ffs(msk) - 1][lane] + 1);
+            for (uint32_t msk = sL.lt_mask; msk; msk &= msk - 1) hi = min(hi, sm_m[warp][__ffs(msk) - 1][lane]);
+            const uint32_t *lst = g.adj + moff;
+            s0 = lo ? lbound(lst, mdeg, lo) : 0;
+            e0 = hi != kFullMask ? lbound(lst, mdeg, hi) : mdeg;
+            if (e0 < s0) e0 = s0;
+            if (need_ub)
+                for (uint32_t t = 0; t < sN.nj; ++t)
+                    if (sN.jpos[t] < lvl) {
+                        const uint32_t u = sm_m[warp][sN.jpos[t]][lane];
+                        ubp = min(ubp, (sN.jdir[t] ? g.in_info[u] : g.out_info[u]).y);
+                    }
+            if (MODE == kBytesMode) local += bytes + 8;
+            if (closed) {
+                // one list, no signature: the window minus the matched vertices in it
+                uint32_t sub = 0;
+                for (uint32_t j = 0; j < lvl; ++j) {
+                    const uint32_t mj = sm_m[warp][j][lane];
+                    if (mj >= lo && mj < hi && contains(lst, mdeg, mj)) ++sub;
+                }
+                local += (e0 - s0) - sub;
+            }
+        }
+        if (MODE == kBytesMode || closed) continue;
+        __syncwarp();
+        // concatenated candidate sequence of the 32 parents
+        const uint32_t len = e0 - s0;
+        uint32_t incl = len;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t ftotal = __shfl_sync(kFullMask, incl, 31);
+        for (uint32_t f0 = 0; f0 < ftotal; f0 += 32) {
+            const uint32_t f = f0 + lane;
+            // owner = number of lanes whose inclusive end is <= f
+            uint32_t owner = 0;
+            #pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const uint32_t probe = __shfl_sync(kFullMask, incl, int(owner + step - 1));
+                if (probe <= f) owner += step;
+            }
+            owner = min(owner, 31u);
+            const uint32_t o_incl = __shfl_sync(kFullMask, incl, int(owner));
+            const uint32_t o_len = __shfl_sync(kFullMask, len, int(owner));
+            const uint32_t o_s0 = __shfl_sync(kFullMask, s0, int(owner));
+            const uint32_t o_moff = __shfl_sync(kFullMask, moff, int(owner));
+            const uint32_t o_tmin = __shfl_sync(kFullMask, tmin, int(owner));
+            const uint32_t o_ubp = __shfl_sync(kFullMask, ubp, int(owner));
+            bool ok = f < ftotal;
+            const uint32_t idx = o_s0 + (f - (o_incl - o_len));
+            const uint32_t c = ok ? __ldg(g.adj + o_moff + idx) : 0;
+            if (ok)
+                for (uint32_t j = 0; j < lvl; ++j)
+                    if (c == sm_m[warp][j][owner]) { ok = false; break; }
+            uint2 co = make_uint2(0, 0), ci = make_uint2(0, 0);
+            if (ok && load_info) {
+                co = g.out_info[c];
+                ci = sym ? co : g.in_info[c];
+            }
+            if (ok && check_sig) ok = ci.y >= sL.qin && co.y >= sL.qout;
+            if (ok)
+                for (uint32_t t = 0; t < nj; ++t) {
+                    if (t == o_tmin) continue;
+                    if (!contains(g.adj + sm_off[warp][t][owner], sm_deg[warp][t][owner], c)) { ok = false; break; }
+                }
+            if constexpr (MODE == kCountMode) {
+                local += ok;
+            } else {
+                uint32_t ub = o_ubp;
+                if (ub_out) ub = min(ub, co.y);
+                if (ub_in) ub = min(ub, ci.y);
+                const unsigned m = __ballot_sync(kFullMask, ok);
+                const uint32_t nn = __popc(m);
+                if (obn + nn > uint32_t(kOutBuf)) flush();
+                if (ok) {
+                    const uint32_t r = obn + __popc(m & lanemask_lt);
+                    ob_v[warp][r] = c;
+                    ob_p[warp][r] = pa + start + owner;
+                    ob_u[warp][r] = ub;
+                }
+                obn += nn;
+            }
+        }
+        __syncwarp();
+    }
+    if constexpr (MODE == kExpand) {
+        if (obn) flush();
+    } else {
+        #pragma unroll
+        for (int s = 16; s; s >>= 1) local += __shfl_xor_sync(kFullMask, local, s);
+        if (lane == 0 && local) atomicAdd(acc, local);
+    }
+}
+
 // ---- chunk planner ------------------------------------------------------
 // Tile sums of the child bounds of parents [pa, pb).
 __global__ void k_tile_sums(const uint32_t *__restrict__ ub, uint32_t pa, uint32_t pb,
@@ -412,6 +623,9 @@ k_plan(const uint64_t *__restrict__ tsum, uint32_t ntiles, unsigned long long ca
 
 int g_num_sms = 0;
 int g_level_blocks[3] = {0, 0, 0};
+int g_flat_blocks[3] = {0, 0, 0};
+// CUTS_LEVEL_KERNEL=warp selects the warp-per-parent form (A/B comparisons)
+bool g_use_flat = true;
 
 int launch_geometry() {
     if (g_num_sms) return CUTS_OK;
@@ -425,6 +639,14 @@ int launch_geometry() {
     g_level_blocks[kCountMode] = std::max(1, b) * g_num_sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level<kBytesMode>, kWarps * 32, 0));
     g_level_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level_flat<kExpand>, kFW * 32, 0));
+    g_flat_blocks[kExpand] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level_flat<kCountMode>, kFW * 32, 0));
+    g_flat_blocks[kCountMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level_flat<kBytesMode>, kFW * 32, 0));
+    g_flat_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
+    const char *kv = std::getenv("CUTS_LEVEL_KERNEL");
+    g_use_flat = !(kv && std::strcmp(kv, "warp") == 0);
     return CUTS_OK;
 }
 
@@ -519,6 +741,7 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     want = std::min(want, 64.0 * (1ull << 30));
     want = std::min(want, 0.6 * double(freeb));
     g->arena_bytes = size_t(want);
+    g->arena_default = g->arena_bytes;
     *out = g;
     return CUTS_OK;
 }
@@ -629,9 +852,12 @@ struct Run {
         uint32_t *out_n = g.d_u32 + kSlotOut + lvl;
         if (mode == kExpand) CK(cudaMemsetAsync(out_n, 0, sizeof(uint32_t), g.stream));
         const uint32_t work = pb - pa;
-        const uint32_t warps_needed = (work + grain - 1) / grain;
-        uint32_t blocks = std::min<uint32_t>(uint32_t(g_level_blocks[mode]),
-                                             (warps_needed + kWarps - 1) / kWarps);
+        const bool flat = g_use_flat && hp->plan.lv[lvl].nj <= uint32_t(kFJ);
+        const uint32_t per_warp = flat ? 32 : grain;
+        const uint32_t wpb = flat ? kFW : kWarps;
+        const uint32_t warps_needed = (work + per_warp - 1) / per_warp;
+        uint32_t blocks = std::min<uint32_t>(uint32_t(flat ? g_flat_blocks[mode] : g_level_blocks[mode]),
+                                             (warps_needed + wpb - 1) / wpb);
         blocks = std::max<uint32_t>(blocks, 1);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile) {
@@ -639,7 +865,18 @@ struct Run {
             CK(cudaEventCreate(&e1));
             CK(cudaEventRecord(e0, g.stream));
         }
-        if (mode == kExpand)
+        if (flat) {
+            unsigned long long *acc = mode == kBytesMode ? g.d_u64 + 2 : g.d_u64;
+            if (mode == kExpand)
+                k_level_flat<kExpand><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
+                    g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, acc);
+            else if (mode == kCountMode)
+                k_level_flat<kCountMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc);
+            else
+                k_level_flat<kBytesMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc);
+        } else if (mode == kExpand)
             k_level<kExpand><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
                 g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, g.d_u64);
         else if (mode == kCountMode)

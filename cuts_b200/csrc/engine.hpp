@@ -26,6 +26,7 @@ struct DeviceGraph {
     // trie-level arena, carved per query
     void *arena = nullptr;
     size_t arena_bytes = 0;
+    size_t arena_default = 0;
     uint64_t level_cap_req = 0;   // 0 = automatic
 
     // small device scratch and pinned host mirrors

@@ -43,37 +43,39 @@ static double frac_ge(const std::vector<uint64_t> &ge, uint64_t n, uint32_t d) {
 
 static float logf20(double x) { return float(std::log(std::max(x, 1e-12)) / 20.0); }
 
-// Features of position i of `order` (prefix order[0..i]); parent_log =
-// log(1 + |L_{i-1}|) (true sizes when training, predictions when searching).
-void step_features(const Query &q, const DegreeStats &ds, const uint32_t *order, uint32_t i,
-                   float parent_log, float *f) {
+// Undirected neighbour masks and degrees of the query (self-loops excluded).
+struct QMasks {
+    uint32_t nb[kMaxK];
+    uint32_t deg[kMaxK];
+};
+static QMasks masks_of(const Query &q) {
+    QMasks m{};
+    for (uint32_t v = 0; v < q.k; ++v) {
+        for (uint32_t w : q.out[v]) if (w != v) m.nb[v] |= 1u << w;
+        for (uint32_t w : q.in[v]) if (w != v) m.nb[v] |= 1u << w;
+    }
+    for (uint32_t v = 0; v < q.k; ++v) m.deg[v] = uint32_t(__builtin_popcount(m.nb[v]));
+    return m;
+}
+
+static void features_masked(const Query &q, const QMasks &M, const DegreeStats &ds,
+                            const uint32_t *order, uint32_t i, float parent_log, float *f) {
     const uint32_t v = order[i];
     std::fill(f, f + kFeatures, 0.f);
-    std::vector<char> nb(q.k, 0);
-    for (uint32_t w : q.out[v]) nb[w] = 1;
-    for (uint32_t w : q.in[v]) nb[w] = 1;
-    uint32_t qdeg = 0;
-    for (uint32_t w = 0; w < q.k; ++w) qdeg += (w != v) && nb[w];
-    uint32_t nj = 0, minjdeg = 1000;
-    for (uint32_t j = 0; j < i; ++j) {
-        const uint32_t u = order[j];
-        if (nb[u] && u != v) {
-            ++nj;
-            uint32_t du = 0;
-            std::vector<char> nu(q.k, 0);
-            for (uint32_t w : q.out[u]) nu[w] = 1;
-            for (uint32_t w : q.in[u]) nu[w] = 1;
-            for (uint32_t w = 0; w < q.k; ++w) du += (w != u) && nu[w];
-            minjdeg = std::min(minjdeg, du);
-        }
-    }
+    uint32_t prefix = 0;
+    for (uint32_t j = 0; j < i; ++j) prefix |= 1u << order[j];
+    const uint32_t joined = M.nb[v] & prefix;
+    const uint32_t nj = uint32_t(__builtin_popcount(joined));
+    uint32_t minjdeg = 1000;
+    for (uint32_t msk = joined; msk; msk &= msk - 1) minjdeg = std::min(minjdeg, M.deg[__builtin_ctz(msk)]);
     uint32_t inner = 0;  // undirected query edges within positions 0..i
-    for (uint32_t a = 0; a <= i; ++a)
-        for (uint32_t b = a + 1; b <= i; ++b)
-            inner += q.has_arc(order[a], order[b]) || q.has_arc(order[b], order[a]);
+    const uint32_t upto = prefix | (1u << v);
+    for (uint32_t msk = upto; msk; msk &= msk - 1)
+        inner += uint32_t(__builtin_popcount(M.nb[__builtin_ctz(msk)] & upto));
+    inner /= 2;
     const double surv = std::min(frac_ge(ds.out_ge, ds.n, uint32_t(q.out[v].size())),
                                  frac_ge(ds.in_ge, ds.n, uint32_t(q.in[v].size())));
-    f[0] = qdeg / 8.f;
+    f[0] = M.deg[v] / 8.f;
     f[1] = nj / 4.f;
     f[2] = i / 8.f;
     f[3] = q.k / 8.f;
@@ -83,8 +85,14 @@ void step_features(const Query &q, const DegreeStats &ds, const uint32_t *order,
     f[7] = inner / 16.f;
     f[8] = (nj ? minjdeg : 0) / 8.f;
     f[9] = float(std::log1p(double(ds.n)) / 20.0);
-    for (int b = 1; b <= 6; ++b)
-        f[9 + b] = logf20(frac_ge(ds.out_ge, ds.n, 1u << (2 * b)));
+    for (int b = 1; b <= 6; ++b) f[9 + b] = logf20(frac_ge(ds.out_ge, ds.n, 1u << (2 * b)));
+}
+
+// Features of position i of `order` (prefix order[0..i]); parent_log =
+// log(1 + |L_{i-1}|) (true sizes when training, predictions when searching).
+void step_features(const Query &q, const DegreeStats &ds, const uint32_t *order, uint32_t i,
+                   float parent_log, float *f) {
+    features_masked(q, masks_of(q), ds, order, i, parent_log, f);
 }
 
 static uint32_t joins_at(const Query &q, const uint32_t *order, uint32_t i) {
@@ -121,6 +129,7 @@ int learned_order(const Query &q, const DegreeStats &ds, Mlp &mlp, const OrderSe
     out.order = score;
     if (k <= 2) return CUTS_OK;
     const size_t beam = opt.beam ? opt.beam : 100000;
+    const QMasks M = masks_of(q);
     std::vector<Cand> cur;
     for (uint32_t v = 0; v < k; ++v) {
         Cand c;
@@ -145,7 +154,7 @@ int learned_order(const Query &q, const DegreeStats &ds, Mlp &mlp, const OrderSe
         feats.assign(rows.size() * kFeatures, 0.f);
         for (size_t r = 0; r < rows.size(); ++r) {
             const float parent = i ? rows[r]->pred[i - 1] : 0.f;
-            step_features(q, ds, rows[r]->order.data(), i, parent, &feats[r * kFeatures]);
+            features_masked(q, M, ds, rows[r]->order.data(), i, parent, &feats[r * kFeatures]);
         }
         std::vector<float> y(rows.size());
         rc = mlp.predict(feats.data(), int(rows.size()), y.data());
@@ -158,9 +167,7 @@ int learned_order(const Query &q, const DegreeStats &ds, Mlp &mlp, const OrderSe
         for (auto &c : cur) {
             for (uint32_t v = 0; v < k; ++v) {
                 if (c.used >> v & 1) continue;
-                bool joined = false;
-                for (uint32_t u : c.order) joined |= q.has_arc(u, v) || q.has_arc(v, u);
-                if (!joined) continue;
+                if (!(M.nb[v] & c.used)) continue;
                 Cand n2 = c;
                 n2.order.push_back(v);
                 n2.used |= 1u << v;

@@ -102,6 +102,11 @@ int cuts_graph_info(cuts_graph g, uint32_t *n, uint64_t *arcs, int *symmetric,
  * fixed GPU_TABLE_LIMIT (common.h:25, gpu_memory_allocation.cu:56-59). */
 int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries);
 
+/* Size in bytes of the trie-level arena (allocated at the first count; 0 =
+ * automatic: 384 B per arc within [256 MB, 64 GB] and 60% of free memory).
+ * Frees the current arena; the next count allocates the new size. */
+int cuts_graph_set_arena_bytes(cuts_graph g, uint64_t bytes);
+
 void cuts_graph_free(cuts_graph g);
 
 /* ---- query graph -------------------------------------------------- */

@@ -381,9 +381,28 @@ static int make_plan(const or_graph *d, const or_graph *q, const uint32_t *order
     return OR_OK;
 }
 
+static int count_impl(const or_graph *d, const or_graph *q, const uint32_t *order_in,
+                      uint32_t root_begin, uint32_t root_end, uint32_t shard, uint32_t nshards,
+                      int nthreads, uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes);
+
 int or_count(const or_graph *d, const or_graph *q, const uint32_t *order_in,
              uint32_t root_begin, uint32_t root_end, int nthreads,
              uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes) {
+    return count_impl(d, q, order_in, root_begin, root_end, 0, 1, nthreads, count, level_sizes,
+                      alg_bytes);
+}
+
+int or_count_striped(const or_graph *d, const or_graph *q, const uint32_t *order,
+                     uint32_t shard, uint32_t nshards, int nthreads, uint64_t *count,
+                     uint64_t *level_sizes) {
+    if (nshards == 0 || shard >= nshards) return OR_ERR_QUERY;
+    return count_impl(d, q, order, 0, UINT32_MAX, shard, nshards, nthreads, count, level_sizes,
+                      NULL);
+}
+
+static int count_impl(const or_graph *d, const or_graph *q, const uint32_t *order_in,
+                      uint32_t root_begin, uint32_t root_end, uint32_t shard, uint32_t nshards,
+                      int nthreads, uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes) {
     plan_t P;
     uint32_t order[OR_MAX_QUERY];
     int rc = make_plan(d, q, order_in, &P, order);
@@ -394,7 +413,7 @@ int or_count(const or_graph *d, const or_graph *q, const uint32_t *order_in,
     if (!roots) return OR_ERR_NOMEM;
     uint64_t nr = 0;
     for (uint32_t u = 0; u < d->n; ++u)
-        if (sig_ok(&P, 0, u)) roots[nr++] = u;
+        if (u % nshards == shard && sig_ok(&P, 0, u)) roots[nr++] = u;
     uint64_t rb = root_begin < nr ? root_begin : nr;
     uint64_t re = root_end < nr ? root_end : nr;
     uint64_t lvl[OR_MAX_QUERY] = {0};

@@ -51,6 +51,7 @@ def lib():
         L.or_joins_for_order.argtypes = [gp, u32p, u32p, u32p, u32p, u32p]
         L.or_count.argtypes = [gp, gp, u32p, C.c_uint32, C.c_uint32, C.c_int, u64p, u64p, u64p]
         L.or_enumerate.argtypes = [gp, gp, u32p, _CB, C.c_void_p]
+        L.or_count_striped.argtypes = [gp, gp, u32p, C.c_uint32, C.c_uint32, C.c_int, u64p, u64p]
         _lib = L
     return _lib
 
@@ -144,6 +145,20 @@ def count(d: Graph, q: Graph, order_: Optional[Sequence[int]] = None, root_begin
     if rc:
         raise ValueError(f"oracle count failed ({rc})")
     return cnt.value, list(lv), by.value
+
+
+def count_striped(d: Graph, q: Graph, shard: int, nshards: int, order_: Optional[Sequence[int]] = None,
+                  nthreads: int = 0):
+    """(count, level_sizes) over the roots u with u % nshards == shard."""
+    k = q.n
+    cnt = C.c_uint64()
+    lv = (C.c_uint64 * k)()
+    op = (C.c_uint32 * k)(*order_) if order_ is not None else None
+    rc = lib().or_count_striped(C.byref(d.g), C.byref(q.g), op, shard, nshards, nthreads,
+                                C.byref(cnt), lv)
+    if rc:
+        raise ValueError(f"oracle striped count failed ({rc})")
+    return cnt.value, list(lv)
 
 
 def enumerate_matches(d: Graph, q: Graph, order_: Optional[Sequence[int]] = None) -> List[tuple]:

@@ -1,0 +1,106 @@
+"""Generate tests/golden/ref_counts.json: counts of the reference binary
+(oracle/_ref/cuts_ref, the unmodified reference built for sm_100a by
+`make -C oracle ref`) on this project's seeded inputs.  Runs on a GPU machine:
+
+    python tests/golden/make_ref_counts.py
+
+Every input is checked safe for the reference before it runs (SURVEY hazards
+H1/H3): maximum degree below its 15,112-entry per-warp candidate helper, and
+level sizes (from this project's oracle) far below its u32 tables and its
+5e10-word final table.  Each case runs `cuts <data> <query>` and
+`cuts <data> <query> 4`; the fixture records the graph and query recipes
+(not their text) with the counts the reference printed.
+"""
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import cuts_b200 as cb  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+HELPER_SAFE_DEGREE = 15000
+GRAPHS = {
+    "er2k": ("er", dict(n=2000, p=10.0 / 1999, seed=3)),
+    "er10k": ("er", dict(n=10000, p=8.0 / 9999, seed=0)),
+    "cl3k": ("cl", dict(n=3000, m=12000, gamma=2.2, wmin=2.0, cap=60.0, seed=8)),
+    "cl5k": ("cl", dict(n=5000, m=20000, gamma=2.1, wmin=2.0, cap=100.0, seed=5)),
+}
+
+
+def make_graph(kind, p):
+    if kind == "er":
+        return cb.HostGraph.erdos_renyi(p["n"], p["p"], p["seed"])
+    return cb.HostGraph.chung_lu(p["n"], p["m"], p["gamma"], p["wmin"], p["cap"], p["seed"])
+
+
+def queries():
+    qs = {name: cb.named_query_arcs(name) for name in
+          ["triangle", "4-cycle", "5-cycle", "house", "4-clique+pendant", "3-prism"]}
+    for s in range(8):
+        k = 4 + s % 3
+        qs[f"rand{k}_{s}"] = (k, cb.random_query_arcs(k, 0.35, 700 + s))
+    # directed queries (orientation of random undirected ones)
+    for s in range(4):
+        k = 3 + s % 3
+        und = cb.random_query_arcs(k, 0.6, 800 + s)
+        qs[f"dir{k}_{s}"] = (k, [a for a in und if (a[0] + a[1] + s) % 3 != 0 or a[0] < a[1]])
+    return qs
+
+
+LINE = re.compile(r"^(.*),(.*),([0-9.e+-]+)ms,(\d+)$")
+
+
+def run_ref(binary, dpath, qpath, trunks=None):
+    cmd = [binary, dpath, qpath] + ([str(trunks)] if trunks else [])
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    for line in r.stdout.splitlines()[::-1]:
+        m = LINE.match(line.strip())
+        if m:
+            return int(m.group(4)), float(m.group(3))
+    raise RuntimeError(f"no result line from {cmd}: rc={r.returncode} {r.stdout[-500:]} {r.stderr[-500:]}")
+
+
+def main():
+    binary = O.REF_CUTS
+    assert os.path.exists(binary), "build it: make -C oracle ref"
+    out = {"generator": "tests/golden/make_ref_counts.py", "binary": "oracle/_ref/cuts_ref",
+           "cases": []}
+    with tempfile.TemporaryDirectory() as d:
+        for gname, (kind, params) in GRAPHS.items():
+            h = make_graph(kind, params)
+            n, arcs, sym, maxd = h.info()
+            assert maxd < HELPER_SAFE_DEGREE, (gname, maxd)
+            dpath = os.path.join(d, gname + ".g")
+            h.write(dpath)
+            oo, oa, _, _ = h.csr()
+            od = O.Graph.from_csr(n, oo, oa)
+            for qname, (k, qarcs) in queries().items():
+                q = cb.Query.from_arcs(k, qarcs)
+                cnt, lv, _ = O.count(od, O.Graph.from_arcs(k, qarcs), q.order)
+                # the reference stores every level of a trunk in one u32 table of
+                # ~3.7e9 words and writes each match into a 5e10-word table
+                if sum(lv[:-1]) > 5e8 or cnt > 5e9:
+                    continue
+                qpath = os.path.join(d, qname + ".g")
+                cb.write_query(qpath, k, qarcs)
+                c1, ms1 = run_ref(binary, dpath, qpath)
+                c4, ms4 = run_ref(binary, dpath, qpath, 4)
+                out["cases"].append({"graph": gname, "graph_kind": kind, "graph_params": params,
+                                     "query": qname, "k": k, "arcs": qarcs, "ref_count": c1,
+                                     "ref_count_trunks4": c4, "ref_ms": ms1, "ref_ms_trunks4": ms4,
+                                     "oracle_count": cnt})
+                print(gname, qname, c1, c4, cnt, f"{ms1:.2f}ms", flush=True)
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_counts.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=0)
+    print(f"wrote {len(out['cases'])} cases to {dst}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,78 @@
+"""The learned order end to end on a GPU: training data from plain runs, the
+model trained by the engine's kernels, the order search, the score-order
+fallback, and what the trained model gains over the method without it."""
+import numpy as np
+import pytest
+
+import cuts_b200 as cb
+from cuts_b200 import learned as L
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    h = cb.HostGraph.chung_lu(3000, 12000, 2.2, 2.0, 60.0, seed=8)
+    g = h.upload(0)
+    train_q = []
+    for s in range(80):
+        k = 4 + s % 3
+        train_q.append((k, cb.random_query_arcs(k, 0.3, 10000 + s)))
+    samples = L.collect(g, train_q, orders_per_query=5, seed=1)
+    X, y, _ = L.features(g, train_q, samples)
+    model = L.train(X, y, epochs=300, batch=1024, lr=2e-3)
+    eval_q = []
+    for s in range(40):
+        k = 4 + s % 3
+        eval_q.append((k, cb.random_query_arcs(k, 0.3, s)))
+    return g, model, train_q, eval_q, (X, y)
+
+
+def test_model_fits_training_levels(setup):
+    g, model, _, _, (X, y) = setup
+    assert L.prediction_error(model, X, y) < 1.0  # nats, teacher forced
+
+
+def test_learned_order_keeps_counts_and_gains(setup):
+    """Order never changes the count; the learned orders do less measured work
+    than the score orders over the held-out queries (the score order is the
+    fallback, so no query may get much worse)."""
+    g, model, _, eval_q, _ = setup
+    w_score = w_learned = 0.0
+    switched = 0
+    for k, arcs in eval_q:
+        q = cb.Query.from_arcs(k, arcs)
+        rs = g.count(q, stats=True)
+        ws = L.work(rs.level_sizes, k, L.joins_of(q))
+        order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model)
+        rl = g.count(q, stats=True)
+        wl = L.work(rl.level_sizes, k, L.joins_of(q))
+        assert rl.count == rs.count
+        w_score += ws
+        w_learned += wl
+        switched += pw < sw
+    print(f"held-out work: score {w_score:.3e}, learned {w_learned:.3e}, "
+          f"gain {w_score / max(w_learned, 1):.2f}x, {switched}/{len(eval_q)} orders changed")
+    assert w_learned <= w_score
+
+
+def test_fallback_without_model(setup):
+    g, _, _, eval_q, _ = setup
+    k, arcs = eval_q[0]
+    q = cb.Query.from_arcs(k, arcs)
+    score = q.order
+    order, _, _ = q.plan(g, cb.ORDER_LEARNED, None)
+    assert order == score
+
+
+def test_score_order_judges_predictions(setup):
+    """Prediction error of the model on the score orders of held-out queries
+    (measured sizes vs teacher-forced predictions) stays bounded."""
+    g, model, _, eval_q, _ = setup
+    samples = []
+    for i, (k, arcs) in enumerate(eval_q[:20]):
+        q = cb.Query.from_arcs(k, arcs)
+        lv, ms = L.level_sizes(g, q, 1)
+        samples.append(L.Sample(i, q.order, lv, ms, True))
+    X, y, _ = L.features(g, eval_q, samples)
+    assert L.prediction_error(model, X, y) < 1.5
