@@ -443,8 +443,27 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                         const uint32_t u = sm_m[warp][sN.jpos[t]][lane];
                         ubp = min(ubp, (sN.jdir[t] ? g.in_info[u] : g.out_info[u]).y);
                     }
-            if (MODE == kBytesMode) local += bytes + 8;
-            if (closed) {
+            if (MODE == kBytesMode) {
+                // what this kernel's algorithm reads for the parent: its own
+                // and its ancestors' (vertex, parent) entries, the joined
+                // vertices' info, then either the closed form's probes or the
+                // streamed candidate window plus, per candidate, the signature
+                // gather and one lower-bound probe sequence per other list
+                (void)bytes;
+                auto probes = [](uint32_t len) { return 32u - __clz(len | 1u); };
+                unsigned long long b = 8ull * lvl + 8ull * nj;
+                const uint32_t len = e0 - s0;
+                if (sL.closed_form) {  // the count kernel's closed form
+                    b += 4ull * lvl * probes(mdeg);
+                } else {
+                    uint32_t per = check_sig ? 8 : 0;
+                    for (uint32_t t = 0; t < nj; ++t)
+                        if (t != tmin) per += 4 * probes(sm_deg[warp][t][lane]);
+                    b += 4ull * len + uint64_t(len) * per;
+                }
+                local += b;
+            }
+            if (closed && MODE == kCountMode) {
                 // one list, no signature: the window minus the matched vertices in it
                 uint32_t sub = 0;
                 for (uint32_t j = 0; j < lvl; ++j) {

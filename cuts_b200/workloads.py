@@ -1,0 +1,83 @@
+"""Seeded workloads beyond the headline benchmark.
+
+* learned: the 1M-vertex power-law graph (exponent 2.1, cap 20,000, 10M
+  edges); 200 random connected queries (5-8 vertices, spanning tree plus
+  extra edges at density 0.3, seeds 0..199); the cost model trained on
+  per-level sizes of 2,000 other queries (seeds 10,000..11,999); plain
+  (score order, one query at a time) against learned order + one batched
+  launch.
+* batched: a 4M-vertex power-law graph (exponent 2.2, 40M edges, cap
+  20,000); 4,096 random connected queries of 3-7 vertices, density
+  0.2-0.6, in one persistent CUDA-graph launch, launch shape autotuned.
+* large: a 16M-vertex power-law graph (exponent 2.1, cap 100,000, 256M
+  edges, ~2 GB int32 CSR); 6-cycle, 3-prism and a seeded random 6-vertex /
+  8-edge query in 8 chunks.
+
+Queries whose exact count does not finish within the stated time budget are
+reported as unfinished, never as a count.
+"""
+from __future__ import annotations
+
+import math
+import time
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+import cuts_b200 as cb
+from cuts_b200 import learned as L
+
+
+def eval_queries(n: int = 200, seed0: int = 0, kmin: int = 5, kmax: int = 8, p: float = 0.3):
+    rng = np.random.default_rng(12345 + seed0)
+    out = []
+    for s in range(n):
+        k = int(rng.integers(kmin, kmax + 1))
+        out.append((k, cb.random_query_arcs(k, p, seed0 + s)))
+    return out
+
+
+def batched_queries(n: int = 4096, seed0: int = 0):
+    rng = np.random.default_rng(777 + seed0)
+    out = []
+    for s in range(n):
+        k = int(rng.integers(3, 8))
+        p = float(rng.uniform(0.2, 0.6))
+        out.append((k, cb.random_query_arcs(k, p, seed0 + s)))
+    return out
+
+
+def graph(name: str) -> "cb.HostGraph":
+    if name == "mid":
+        return cb.HostGraph.chung_lu(1_000_000, 10_000_000, 2.1, 2.0, 20000.0, 0)
+    if name == "batched":
+        return cb.HostGraph.chung_lu(4_000_000, 40_000_000, 2.2, 2.0, 20000.0, 0)
+    if name == "large":
+        return cb.HostGraph.chung_lu(16_000_000, 256_000_000, 2.1, 2.0, 100000.0, 0)
+    raise ValueError(name)
+
+
+def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0):
+    """Score order, one query at a time, each under budget_ms."""
+    res = []
+    t0 = time.perf_counter()
+    for k, arcs in queries:
+        q = cb.Query.from_arcs(k, arcs)
+        r, done = g.count_budget(q, budget_ms, flags=flags)
+        res.append((done, r.count if done else None, r.ms))
+    return res, time.perf_counter() - t0
+
+
+def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 256,
+                epochs: int = 300, seed: int = 10000, time_budget_s: float = 600.0):
+    train_q = eval_queries(n_train, seed0=seed)
+    t0 = time.perf_counter()
+    samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
+                        time_budget_s=time_budget_s)
+    t_collect = time.perf_counter() - t0
+    X, y, _ = L.features(g, train_q, samples)
+    t1 = time.perf_counter()
+    model = L.train(X, y, epochs=epochs, batch=4096, lr=2e-3)
+    t_train = time.perf_counter() - t1
+    return model, {"samples": len(samples), "rows": int(len(y)), "collect_s": t_collect,
+                   "train_s": t_train, "fit_mae_nats": L.prediction_error(model, X, y)}
