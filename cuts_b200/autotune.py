@@ -26,6 +26,15 @@ def tune_batch(g: "cb.Graph", queries: Sequence["cb.Query"], flags: int = 0,
     """Returns (best (grain, grab, blocks), {config: median ms})."""
     times: Dict[Tuple[int, int, int], float] = {}
     ref: Optional[List[int]] = None
+    if budget_ms > 0:
+        # tune on the queries that finish within the budget in the default shape
+        b = g.batch(queries, flags=flags)
+        _, status, _ = b.run(budget_ms)
+        b.close()
+        queries = [q for q, s in zip(queries, status) if s == 0]
+        budget_ms = 0.0
+        if not queries:
+            return (64, 1, 0), times
     for gr in grains:
         for tg in grabs:
             for bl in blocks:

@@ -337,7 +337,8 @@ template <int MODE>
 __global__ void __launch_bounds__(kFW * 32)
 k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, uint32_t pb,
              uint32_t *__restrict__ cursor, uint32_t *__restrict__ out_n, uint32_t out_cap,
-             uint32_t *__restrict__ err, unsigned long long *__restrict__ acc) {
+             uint32_t *__restrict__ err, unsigned long long *__restrict__ acc,
+             unsigned long long *__restrict__ acc2) {
     __shared__ LevelPlan sL, sN;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
@@ -378,8 +379,13 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     const bool check_sig = sL.check_sig != 0;
     const bool load_info = check_sig || ub_out || ub_in;
     const bool closed = MODE == kCountMode && sL.closed_form;
+    // level k-2 counting level k-1 too: each candidate c adds the last
+    // level's closed form, |window of L| - matched vertices in it, where L
+    // is an earlier vertex's list and c itself is one of the matched
+    const bool fold = MODE != kExpand && sL.fold;
+    const bool fold_guar_c = fold && ((sN.guar_mask >> lvl) & 1u);
     const uint32_t total = pb - pa;
-    unsigned long long local = 0;
+    unsigned long long local = 0, local2 = 0;
     uint32_t obn = 0;
 
     auto flush = [&]() {
@@ -418,6 +424,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
         }
         // joined lists, shortest first
         uint32_t moff = 0, mdeg = 0, tmin = 0, s0 = 0, e0 = 0, ubp = kFullMask;
+        uint32_t f_off = 0, f_deg = 0, f_lo = 0, f_hi = kFullMask, f0 = 0;
         unsigned long long bytes = 0;
         if (have) {
             mdeg = kFullMask;
@@ -443,6 +450,23 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                         const uint32_t u = sm_m[warp][sN.jpos[t]][lane];
                         ubp = min(ubp, (sN.jdir[t] ? g.in_info[u] : g.out_info[u]).y);
                     }
+            if (fold) {
+                const uint32_t u = sm_m[warp][sN.jpos[0]][lane];
+                const uint2 inf = sN.jdir[0] ? g.in_info[u] : g.out_info[u];
+                f_off = inf.x;
+                f_deg = inf.y;
+                for (uint32_t msk = sN.gt_mask; msk; msk &= msk - 1) f_lo = max(f_lo, sm_m[warp][__ffs(msk) - 1][lane] + 1);
+                for (uint32_t msk = sN.lt_mask; msk; msk &= msk - 1) f_hi = min(f_hi, sm_m[warp][__ffs(msk) - 1][lane]);
+                const uint32_t *fl = g.adj + f_off;
+                const uint32_t ws = f_lo ? lbound(fl, f_deg, f_lo) : 0;
+                const uint32_t we = f_hi != kFullMask ? lbound(fl, f_deg, f_hi) : f_deg;
+                uint32_t sub = 0;
+                for (uint32_t j = 0; j < lvl; ++j) {
+                    const uint32_t mj = sm_m[warp][j][lane];
+                    if (mj >= f_lo && mj < f_hi && (((sN.guar_mask >> j) & 1u) || contains(fl, f_deg, mj))) ++sub;
+                }
+                f0 = (we > ws ? we - ws : 0) - sub;
+            }
             if (MODE == kBytesMode) {
                 // what this kernel's algorithm reads for the parent: its own
                 // and its ancestors' (vertex, parent) entries, the joined
@@ -459,6 +483,10 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                     uint32_t per = check_sig ? 8 : 0;
                     for (uint32_t t = 0; t < nj; ++t)
                         if (t != tmin) per += 4 * probes(sm_deg[warp][t][lane]);
+                    if (fold) {
+                        b += 8 + 4ull * lvl * probes(f_deg);
+                        if (!fold_guar_c) per += 4 * probes(f_deg);
+                    }
                     b += 4ull * len + uint64_t(len) * per;
                 }
                 local += b;
@@ -468,7 +496,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                 uint32_t sub = 0;
                 for (uint32_t j = 0; j < lvl; ++j) {
                     const uint32_t mj = sm_m[warp][j][lane];
-                    if (mj >= lo && mj < hi && contains(lst, mdeg, mj)) ++sub;
+                    if (mj >= lo && mj < hi && (((sL.guar_mask >> j) & 1u) || contains(lst, mdeg, mj))) ++sub;
                 }
                 local += (e0 - s0) - sub;
             }
@@ -518,7 +546,21 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                     if (!contains(g.adj + sm_off[warp][t][owner], sm_deg[warp][t][owner], c)) { ok = false; break; }
                 }
             if constexpr (MODE == kCountMode) {
-                local += ok;
+                if (fold) {
+                    const uint32_t o_f0 = __shfl_sync(kFullMask, f0, int(owner));
+                    const uint32_t o_foff = __shfl_sync(kFullMask, f_off, int(owner));
+                    const uint32_t o_fdeg = __shfl_sync(kFullMask, f_deg, int(owner));
+                    const uint32_t o_flo = __shfl_sync(kFullMask, f_lo, int(owner));
+                    const uint32_t o_fhi = __shfl_sync(kFullMask, f_hi, int(owner));
+                    if (ok) {
+                        const bool hit = c >= o_flo && c < o_fhi &&
+                                         (fold_guar_c || contains(g.adj + o_foff, o_fdeg, c));
+                        local += o_f0 - (hit ? 1u : 0u);
+                        ++local2;
+                    }
+                } else {
+                    local += ok;
+                }
             } else {
                 uint32_t ub = o_ubp;
                 if (ub_out) ub = min(ub, co.y);
@@ -541,8 +583,12 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
         if (obn) flush();
     } else {
         #pragma unroll
-        for (int s = 16; s; s >>= 1) local += __shfl_xor_sync(kFullMask, local, s);
+        for (int s = 16; s; s >>= 1) {
+            local += __shfl_xor_sync(kFullMask, local, s);
+            local2 += __shfl_xor_sync(kFullMask, local2, s);
+        }
         if (lane == 0 && local) atomicAdd(acc, local);
+        if (lane == 0 && local2 && acc2) atomicAdd(acc2, local2);
     }
 }
 
@@ -888,13 +934,13 @@ struct Run {
             unsigned long long *acc = mode == kBytesMode ? g.d_u64 + 2 : g.d_u64;
             if (mode == kExpand)
                 k_level_flat<kExpand><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, acc);
+                    g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, acc, nullptr);
             else if (mode == kCountMode)
                 k_level_flat<kCountMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc);
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, g.d_u64 + 3);
             else
                 k_level_flat<kBytesMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc);
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, nullptr);
         } else if (mode == kExpand)
             k_level<kExpand><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
                 g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, g.d_u64);
@@ -929,7 +975,9 @@ struct Run {
     // Expands parents [pa, pb) of L_{lvl-1}, depth first by chunks.
     int expand(uint32_t lvl, uint32_t pa, uint32_t pb) {
         if (pb <= pa) return CUTS_OK;
-        if (lvl + 1 == k && !dump) {
+        // the last level is counted; with a folded plan, level k-2 counts both
+        const uint32_t count_lvl = (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
+        if (lvl == count_lvl && !dump) {
             int rc = launch_level(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
             return rc;
         }
@@ -997,6 +1045,11 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     std::memset(hp, 0, sizeof(RunParams));
     int rc = build_plan(q, g.symmetric, flags, hp->plan);
     if (rc) return rc;
+    if (k >= 3 && hp->plan.lv[k - 2].fold) {
+        // the folded count runs in the flattened kernel only
+        if (!g_use_flat || hp->plan.lv[k - 2].nj > uint32_t(kFJ)) hp->plan.lv[k - 2].fold = 0;
+        else if (stored == k - 1) stored = k - 2;  // level k-2 is counted, not stored
+    }
     hp->stored = stored;
     if (!g.arena) {
         cudaError_t e = cudaMalloc(&g.arena, g.arena_bytes);
@@ -1143,6 +1196,10 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     CK(cudaEventElapsedTime(&res.ms, g.ev0, g.ev1));
     const uint64_t raw = k >= 2 ? uint64_t(g.h_u64[0]) : 0;
     res.level_sizes[k - 1] = k >= 2 ? raw : n0;
+    if (k >= 3 && hp->plan.lv[k - 2].fold) {
+        CK(cudaMemcpy(g.h_u64 + 3, g.d_u64 + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        res.level_sizes[k - 2] = g.h_u64[3];
+    }
     res.count = raw * hp->plan.aut;
     if (opt.want_bytes && k >= 2 && n0 > 0) {
         // untimed second pass: algorithmic bytes of the last-level kernel

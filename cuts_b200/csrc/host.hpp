@@ -91,7 +91,11 @@ struct LevelPlan {
     uint32_t gt_mask;         // c > m_j required for positions j in mask
     uint32_t lt_mask;         // c < m_j required for positions j in mask
     uint32_t closed_form;     // last level: count by list arithmetic
-    uint32_t pad;
+    uint32_t fold;            // level k-2: also counts level k-1 (closed form
+                              // independent of this level's vertex)
+    uint32_t guar_mask;       // last level: positions whose vertex the query's
+                              // own arcs guarantee to be in the joined list
+    uint32_t pad2[3];
     uint8_t jpos[kMaxJ];      // joined position j
     uint8_t jdir[kMaxJ];      // 0: out-list of m_j (P join), 1: in-list (C join)
 };

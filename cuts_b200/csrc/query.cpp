@@ -281,6 +281,18 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
         L.check_sig = (i + 1 < k) || q.self_loop(v);
         L.closed_form = (k >= 2 && i + 1 == k && nj == 1 && !L.check_sig &&
                          !(flags & CUTS_FLAG_NO_CLOSED_FORM));
+        if (L.closed_form) {
+            // m_j lies in the joined list whenever the query has the arc the
+            // list stands for (or its reverse on a symmetric data graph)
+            const uint32_t jp = L.jpos[0], a = q.order[jp];
+            for (uint32_t j = 0; j < i; ++j) {
+                if (j == jp) continue;  // a query self-loop is not a data constraint
+                const uint32_t b = q.order[j];
+                const bool fwd = L.jdir[0] == 0 ? q.has_arc(a, b) : q.has_arc(b, a);
+                const bool rev = L.jdir[0] == 0 ? q.has_arc(b, a) : q.has_arc(a, b);
+                if (fwd || (data_symmetric && rev)) L.guar_mask |= 1u << j;
+            }
+        }
     }
     if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && k >= 2) {
         std::vector<uint32_t> pos(k);
@@ -294,6 +306,15 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
             else plan.lv[pa].lt_mask |= 1u << pb;
         }
         plan.aut = aut;
+    }
+    // Fold the last level into level k-2 when its closed form does not
+    // depend on the vertex chosen at k-2: the joined list is an earlier
+    // position's and no symmetry condition involves position k-2.  Each
+    // level k-2 candidate then contributes the closed form directly.
+    if (k >= 3 && plan.lv[k - 1].closed_form) {
+        const LevelPlan &F = plan.lv[k - 1];
+        const uint32_t pen = 1u << (k - 2);
+        if (F.jpos[0] != k - 2 && !(F.gt_mask & pen) && !(F.lt_mask & pen)) plan.lv[k - 2].fold = 1;
     }
     return CUTS_OK;
 }

@@ -81,3 +81,57 @@ def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, s
     t_train = time.perf_counter() - t1
     return model, {"samples": len(samples), "rows": int(len(y)), "collect_s": t_collect,
                    "train_s": t_train, "fit_mae_nats": L.prediction_error(model, X, y)}
+
+
+def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 5000.0,
+                model=None, train_budget_s: float = 600.0, flags: int = 0):
+    """Plain (score order, one query at a time) vs learned order + one batched
+    launch on the same 200 queries, both under the same per-query budget
+    (the batched launch gets budget_ms x n_eval in total)."""
+    info = {}
+    if model is None:
+        model, info = train_model(g, n_train=n_train, time_budget_s=train_budget_s)
+    qdefs = eval_queries(n_eval)
+    plain, plain_s = plain_pass(g, qdefs, budget_ms, flags)
+    t0 = time.perf_counter()
+    qs = []
+    switched = 0
+    for k, arcs in qdefs:
+        q = cb.Query.from_arcs(k, arcs)
+        _, pw, sw = q.plan(g, cb.ORDER_LEARNED, model)
+        switched += pw < sw
+        qs.append(q)
+    plan_s = time.perf_counter() - t0
+    b = g.batch(qs, flags=flags)
+    counts, status, ms = b.run(budget_ms * n_eval)
+    learned_s = plan_s + ms / 1e3
+    done_p = [d for d, _, _ in plain]
+    done_l = [s == 0 for s in status]
+    agree = all(c == pc for (d, pc, _), c, s in zip(plain, counts, status) if d and s == 0)
+    return {
+        "queries": n_eval, "budget_ms_per_query": budget_ms,
+        "plain": {"finished": sum(done_p), "seconds": plain_s,
+                  "queries_per_s": sum(done_p) / plain_s},
+        "learned_batched": {"finished": sum(done_l), "seconds": learned_s, "plan_s": plan_s,
+                            "launch_ms": ms, "queries_per_s": sum(done_l) / learned_s,
+                            "orders_changed": switched},
+        "counts_agree_where_both_finished": agree,
+        "training": info,
+    }
+
+
+def run_batched(g: "cb.Graph", n: int = 4096, budget_ms: float = 60000.0, tune_sample: int = 256,
+                flags: int = 0):
+    """4,096 queries in one persistent launch; shape autotuned on a sample."""
+    from cuts_b200 import autotune
+    qdefs = batched_queries(n)
+    qs = [cb.Query.from_arcs(k, a) for k, a in qdefs]
+    t0 = time.perf_counter()
+    best, times = autotune.tune_batch(g, qs[:tune_sample], flags=flags, budget_ms=2000.0)
+    tune_s = time.perf_counter() - t0
+    b = g.batch(qs, flags=flags, grain=best[0], tasks_per_grab=best[1], blocks_per_sm=best[2])
+    counts, status, ms = b.run(budget_ms)
+    fin = sum(1 for s in status if s == 0)
+    return {"queries": n, "finished": fin, "launch_ms": ms, "queries_per_s": fin / (ms / 1e3),
+            "tuned": list(best), "tune_s": tune_s, "tasks": b.info()[0],
+            "matches_finished": int(sum(c for c, s in zip(counts, status) if s == 0))}

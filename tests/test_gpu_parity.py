@@ -218,3 +218,30 @@ def test_sharded_counts_sum(cl5k, name):
     parts = [g.count_sharded(q, r, 3) for r in range(3)]
     assert sum(p.count for p in parts) == full.count
     assert [sum(p.level_sizes[i] for p in parts) for i in range(k)] == full.level_sizes
+
+
+# queries whose last vertex hangs off an earlier one: the last level is a
+# closed form and folds into level k-2 (unless a symmetry condition ties it
+# to the penultimate vertex)
+FOLD_QUERIES = {
+    "star3": (4, [(0, 1), (1, 0), (0, 2), (2, 0), (0, 3), (3, 0)]),
+    "tailed-triangle": (4, [(0, 1), (1, 0), (1, 2), (2, 1), (2, 0), (0, 2), (0, 3), (3, 0)]),
+    "4-clique+pendant": cb.named_query_arcs("4-clique+pendant"),
+    "path4": (4, [(0, 1), (1, 0), (1, 2), (2, 1), (2, 3), (3, 2)]),
+    "directed-fan": (4, [(0, 1), (1, 2), (2, 0), (0, 3)]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FOLD_QUERIES))
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK, cb.FLAG_NO_CLOSED_FORM])
+def test_fold_and_guaranteed_members(er2k, cl5k, name, flags):
+    k, arcs = FOLD_QUERIES[name]
+    for h, g, od in (er2k, cl5k):
+        q = cb.Query.from_arcs(k, arcs)
+        cnt, lv, _ = oracle_count(od, k, arcs, q.order)
+        r = g.count(q, flags=flags, stats=True)
+        assert r.count == cnt
+        if flags != cb.FLAG_SYMMETRY_BREAK:
+            assert r.level_sizes == lv
+        r4 = g.count(q, flags=flags, chunks=3)
+        assert r4.count == cnt
