@@ -75,6 +75,7 @@ _SIGS = {
     "cuts_query_joins": (C.c_int, [_vp, _u32p, _u32p, _u32p, _u32p]),
     "cuts_query_set_order": (C.c_int, [_vp, _u32p]),
     "cuts_query_automorphisms": (C.c_int, [_vp, _u64p]),
+    "cuts_query_plan_levels": (C.c_int, [_vp, C.c_int, C.c_uint32, _u32p, _u64p]),
     "cuts_query_free": (None, [_vp]),
     "cuts_count": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float)]),
     "cuts_count_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float),
@@ -282,6 +283,16 @@ class Query:
         _check(lib().cuts_plan(self._h, graph._h, mode, model._h if model else None, beam, margin,
                                _ptr(o, _u32p), C.byref(pw), C.byref(sw)))
         return [int(x) for x in o], pw.value, sw.value
+
+    def plan_levels(self, data_symmetric: bool = True, flags: int = 0):
+        """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt) and |Aut| used."""
+        k = self.k
+        out = np.zeros(8 * k, np.uint32)
+        aut = C.c_uint64()
+        _check(lib().cuts_query_plan_levels(self._h, int(data_symmetric), flags, _ptr(out, _u32p),
+                                            C.byref(aut)))
+        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt"]
+        return [dict(zip(keys, (int(x) for x in out[8 * i:8 * i + 7]))) for i in range(k)], aut.value
 
     def automorphisms(self) -> int:
         a = C.c_uint64()

@@ -267,6 +267,24 @@ int cuts_query_set_order(cuts_query q, const uint32_t *order) {
     })());
 }
 
+int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,
+                           uint64_t *aut) {
+    if (!q || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        Plan p;
+        int rc = build_plan(q->q, data_symmetric != 0, flags, p);
+        if (rc) return rc;
+        for (uint32_t i = 0; i < q->q.k; ++i) {
+            const LevelPlan &L = p.lv[i];
+            uint32_t *o = out + 8 * i;
+            o[0] = L.nj; o[1] = L.check_sig; o[2] = L.closed_form; o[3] = L.fold;
+            o[4] = L.guar_mask; o[5] = L.gt_mask; o[6] = L.lt_mask; o[7] = 0;
+        }
+        if (aut) *aut = p.aut;
+        return CUTS_OK;
+    })());
+}
+
 int cuts_query_automorphisms(cuts_query q, uint64_t *count) {
     if (!q || !count) return set_error(CUTS_ERR_ARG, "null argument");
     *count = automorphism_count(q->q);

@@ -166,3 +166,40 @@ def test_cli_usage_and_bad_trunks(tmp_path):
     r = subprocess.run([cb.CLI_PATH, "/nonexistent/d.txt", "/nonexistent/q.g"],
                        capture_output=True, text=True)
     assert r.returncode == 255 and "failed" in r.stdout
+
+
+def test_plan_fold_and_guarantees():
+    # 4-clique 0..3 + pendant 4 on 0: the pendant is last, joined to position of 0
+    q = cb.Query.from_arcs(*cb.named_query_arcs("4-clique+pendant"))
+    lv, aut = q.plan_levels(True, 0)
+    k = q.k
+    assert q.order[-1] == 4 and aut == 1
+    last, pen = lv[k - 1], lv[k - 2]
+    assert last["closed"] == 1 and last["sig"] == 0 and pen["fold"] == 1
+    pos0 = q.order.index(0)
+    # every other clique vertex is a query neighbour of 0: guaranteed in N(m0)
+    want = sum(1 << j for j in range(k - 1) if j != pos0)
+    assert last["guar"] == want
+    # intermediate levels keep the signature test; level 0 too
+    assert all(l["sig"] == 1 for l in lv[:-1])
+    # no closed form, no fold
+    lv2, _ = q.plan_levels(True, cb.FLAG_NO_CLOSED_FORM)
+    assert lv2[k - 1]["closed"] == 0 and lv2[k - 2]["fold"] == 0
+    # symmetry breaking on a triangle: constraints, |Aut| = 6, no fold (closed form
+    # needs a single joined list)
+    t = cb.Query.from_arcs(*cb.named_query_arcs("triangle"))
+    lv3, aut3 = t.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
+    assert aut3 == 6 and lv3[2]["closed"] == 0 and lv3[1]["fold"] == 0
+    assert lv3[1]["gt"] | lv3[1]["lt"] and lv3[2]["gt"] | lv3[2]["lt"]
+
+
+def test_plan_directed_guarantees():
+    # directed: 0->1, 1->2, 0->3 ; last vertex 3 joined by out-list of m0; 1 is in
+    # out(m0) (arc 0->1) but 2 is not guaranteed
+    q = cb.Query.from_arcs(4, [(0, 1), (1, 2), (0, 3)])
+    q.set_order([0, 1, 2, 3])
+    lv, _ = q.plan_levels(False, 0)
+    assert lv[3]["closed"] == 1
+    assert lv[3]["guar"] == 0b010
+    lv_sym, _ = q.plan_levels(True, 0)
+    assert lv_sym[3]["guar"] == 0b010  # 2 is not adjacent to 0 at all
