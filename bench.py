@@ -175,6 +175,54 @@ def cpu_sample(h, queries, budget_s=20.0):
     return total_cnt / max(total_t, 1e-9), cores, "; ".join(parts)
 
 
+REF_SAFE_DEGREE = 32768 + 112   # cuts_ref_b148: per-warp helper of 32,768 words past 112 in smem
+REF_TABLE_WORDS = 3.5e9          # its trie table (u32 words, every level of a trunk)
+REF_FINAL_WORDS = 4.5e10         # its managed final table
+
+
+def reference_gpu(h, queries, level_sizes, counts, chunks):
+    """Time the reference binary (built for sm_100a, 148-SM grid, enlarged
+    candidate helper) on the workload's queries that it can run without
+    overflowing its fixed tables; the others are reported as unsafe and not
+    launched.  Returns {query: {...}}."""
+    import re
+    import tempfile
+    from oracle import oracle as O
+    binary = O.REF_CUTS.replace("cuts_ref", "cuts_ref_b148")
+    out = {}
+    if not os.path.exists(binary):
+        return {"unavailable": "oracle/_ref/cuts_ref_b148 not built"}
+    n, arcs, sym, maxd = h.info()
+    with tempfile.TemporaryDirectory() as d:
+        dpath = os.path.join(d, "data.g")
+        h.write(dpath)
+        import cuts_b200 as cb
+        for (name, k, qarcs), lv, cnt in zip(queries, level_sizes, counts):
+            stored = sum(lv[:-1])
+            final_words = cnt + (k - 1) * (lv[-2] if k >= 2 else 0)
+            if maxd >= REF_SAFE_DEGREE or stored > REF_TABLE_WORDS or final_words > REF_FINAL_WORDS:
+                out[name] = {"run": False, "reason": f"would overflow the reference's fixed tables "
+                                                     f"(levels {stored:.3g} words, final {final_words:.3g})"}
+                continue
+            qpath = os.path.join(d, name + ".g")
+            cb.write_query(qpath, k, qarcs)
+            t0 = time.perf_counter()
+            r = subprocess.run([binary, dpath, qpath, str(chunks)], capture_output=True, text=True,
+                               timeout=1800)
+            wall = time.perf_counter() - t0
+            m = None
+            for line in r.stdout.splitlines()[::-1]:
+                m = re.match(r"^(.*),(.*),([0-9.e+-]+)ms,(\d+)$", line.strip())
+                if m:
+                    break
+            if not m:
+                out[name] = {"run": True, "failed": (r.stdout + r.stderr)[-300:]}
+                continue
+            out[name] = {"run": True, "ms": float(m.group(3)), "count": int(m.group(4)),
+                         "count_matches": int(m.group(4)) == cnt, "wall_s_with_load": wall}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = _env_rank()
     if rank != 0:
@@ -204,6 +252,48 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# other configurations (reports, not the headline line)
+# ---------------------------------------------------------------------------
+
+def run_other_workload(args):
+    import torch
+    import cuts_b200 as cb
+    from cuts_b200 import workloads as W
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    name = {"learned": "mid", "batched": "batched", "large": "large"}[args.workload]
+    h = W.graph(name)
+    g = h.upload(0)
+    n, arcs, sym, maxd = h.info()
+    gen_s = time.perf_counter() - t0
+    rep = {"workload": args.workload, "graph": {"n": n, "arcs": arcs, "max_degree": maxd,
+                                                "gen_upload_s": gen_s}}
+    if args.workload == "learned":
+        rep.update(W.run_learned(g, budget_ms=args.budget_ms, flags=args.flags))
+    elif args.workload == "batched":
+        rep.update(W.run_batched(g, flags=args.flags))
+    else:
+        g.set_arena_bytes(48 << 30)
+        res = {}
+        qdefs = [("6-cycle",) + cb.named_query_arcs("6-cycle"), ("3-prism",) + cb.named_query_arcs("3-prism")]
+        rq = None
+        for s in range(1000):  # first seeded connected 6-vertex query with exactly 8 edges
+            a = cb.random_query_arcs(6, 0.3, 5000 + s)
+            if len(a) == 16:
+                rq = ("random6e8", 6, a)
+                break
+        qdefs.append(rq)
+        for qname, k, qarcs in qdefs:
+            q = cb.Query.from_arcs(k, qarcs)
+            r, done = g.count_budget(q, args.budget_ms, chunks=8, flags=args.flags | cb.FLAG_SYMMETRY_BREAK)
+            res[qname] = {"finished": done, "count": r.count if done else None, "ms": r.ms,
+                          "levels": r.level_sizes if done else None}
+        rep["queries"] = res
+    print(json.dumps(rep), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # engine
 # ---------------------------------------------------------------------------
 
@@ -216,9 +306,17 @@ def main():
     ap.add_argument("--flags", type=int, default=0, help="CUTS_FLAG_* bits")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="also time the reference binary where it is safe to run")
+    ap.add_argument("--workload", default="mid", choices=["mid", "learned", "batched", "large"],
+                    help="mid = the headline line; the others print their own report line")
+    ap.add_argument("--budget-ms", type=float, default=5000.0,
+                    help="per-query time budget of the learned / large workloads")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "mid":
+        return run_other_workload(args)
 
     import numpy as np
     import torch
@@ -344,6 +442,13 @@ def main():
                                         budget_s=args.cpu_budget)
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
 
+        ref_gpu = None
+        if args.ref_gpu and world == 1:
+            lvls = []
+            for name, q in queries:
+                lvls.append(g.count(q, chunks=chunks, stats=True).level_sizes)
+            ref_gpu = reference_gpu(h, make_queries(), lvls, counts, chunks)
+
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -363,6 +468,7 @@ def main():
                     "d2h_bytes_per_step": 8 * len(queries),
                     "note": "wall clock: CSR upload + padded layout + 4 counts + count reads"},
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(result), flush=True)
     if pg:

@@ -331,7 +331,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
 // single joined list and no signature are counted by the closed form, one
 // parent per lane.
 constexpr int kFW = 4;    // warps per block
-constexpr int kFJ = 16;   // joined lists per level in this form
+constexpr int kFJ = 8;    // joined lists per level in this form (more: warp-per-parent kernel)
 
 template <int MODE>
 __global__ void __launch_bounds__(kFW * 32)
@@ -424,7 +424,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
         }
         // joined lists, shortest first
         uint32_t moff = 0, mdeg = 0, tmin = 0, s0 = 0, e0 = 0, ubp = kFullMask;
-        uint32_t f_off = 0, f_deg = 0, f_lo = 0, f_hi = kFullMask, f0 = 0;
+        uint32_t f_off = 0, f_deg = 0, f_lo = 0, f_hi = kFullMask, fbase = 0;
         unsigned long long bytes = 0;
         if (have) {
             mdeg = kFullMask;
@@ -465,7 +465,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                     const uint32_t mj = sm_m[warp][j][lane];
                     if (mj >= f_lo && mj < f_hi && (((sN.guar_mask >> j) & 1u) || contains(fl, f_deg, mj))) ++sub;
                 }
-                f0 = (we > ws ? we - ws : 0) - sub;
+                fbase = (we > ws ? we - ws : 0) - sub;
             }
             if (MODE == kBytesMode) {
                 // what this kernel's algorithm reads for the parent: its own
@@ -512,8 +512,9 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
             if (lane >= o) incl += y;
         }
         const uint32_t ftotal = __shfl_sync(kFullMask, incl, 31);
-        for (uint32_t f0 = 0; f0 < ftotal; f0 += 32) {
-            const uint32_t f = f0 + lane;
+        uint32_t gal_owner = kFullMask, gal_pos0 = 0, gal_pos1 = 0;
+        for (uint32_t fstep = 0; fstep < ftotal; fstep += 32) {
+            const uint32_t f = fstep + lane;
             // owner = number of lanes whose inclusive end is <= f
             uint32_t owner = 0;
             #pragma unroll
@@ -540,14 +541,29 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                 ci = sym ? co : g.in_info[c];
             }
             if (ok && check_sig) ok = ci.y >= sL.qin && co.y >= sL.qout;
-            if (ok)
+            if (owner != gal_owner) {  // new parent for this lane: restart the searches
+                gal_owner = owner;
+                gal_pos0 = gal_pos1 = 0;
+            }
+            if (ok) {
+                uint32_t r = 0;
                 for (uint32_t t = 0; t < nj; ++t) {
                     if (t == o_tmin) continue;
-                    if (!contains(g.adj + sm_off[warp][t][owner], sm_deg[warp][t][owner], c)) { ok = false; break; }
+                    const uint32_t *lst = g.adj + sm_off[warp][t][owner];
+                    const uint32_t len2 = sm_deg[warp][t][owner];
+                    // this lane's candidates for one parent rise, so its lower
+                    // bounds in each other list rise too: gallop from the last
+                    const uint32_t from = r == 0 ? gal_pos0 : (r == 1 ? gal_pos1 : 0);
+                    const uint32_t pos = lbound_from(lst, len2, from, c);
+                    if (r == 0) gal_pos0 = pos;
+                    else if (r == 1) gal_pos1 = pos;
+                    ++r;
+                    if (pos >= len2 || __ldg(lst + pos) != c) { ok = false; break; }
                 }
+            }
             if constexpr (MODE == kCountMode) {
                 if (fold) {
-                    const uint32_t o_f0 = __shfl_sync(kFullMask, f0, int(owner));
+                    const uint32_t o_fbase = __shfl_sync(kFullMask, fbase, int(owner));
                     const uint32_t o_foff = __shfl_sync(kFullMask, f_off, int(owner));
                     const uint32_t o_fdeg = __shfl_sync(kFullMask, f_deg, int(owner));
                     const uint32_t o_flo = __shfl_sync(kFullMask, f_lo, int(owner));
@@ -555,7 +571,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                     if (ok) {
                         const bool hit = c >= o_flo && c < o_fhi &&
                                          (fold_guar_c || contains(g.adj + o_foff, o_fdeg, c));
-                        local += o_f0 - (hit ? 1u : 0u);
+                        local += o_fbase - (hit ? 1u : 0u);
                         ++local2;
                     }
                 } else {

@@ -31,6 +31,8 @@ def main(argv=None):
     ap.add_argument("--chunks", type=int, default=4)
     ap.add_argument("--flags", type=int, default=0)
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--stripe", type=int, default=1,
+                    help="count only the roots u with u %% stripe == 0 (a smaller case)")
     a = ap.parse_args(argv)
     h = GRAPHS[a.graph]()
     g = h.upload(0)
@@ -48,10 +50,16 @@ def main(argv=None):
                   f"{sum(1 for s in status if s)} unfinished", flush=True)
         return 0
     q = cb.Query.from_arcs(*cb.named_query_arcs(a.query))
-    g.count(q, chunks=a.chunks, flags=a.flags)
+
+    def run():
+        if a.stripe > 1:
+            return g.count_sharded(q, 0, a.stripe, chunks=a.chunks, flags=a.flags)
+        return g.count(q, chunks=a.chunks, flags=a.flags, stats=True)
+
+    run()
     for _ in range(a.repeat):
         t = time.perf_counter()
-        r = g.count(q, chunks=a.chunks, flags=a.flags, stats=True)
+        r = run()
         print(f"{a.query}: count {r.count} in {r.ms:.3f} ms (wall {1e3 * (time.perf_counter() - t):.1f}), "
               f"levels {r.level_sizes}, launches {r.launches}, chunks {r.chunks}", flush=True)
     return 0
