@@ -130,8 +130,14 @@ __device__ unsigned long long count_level(const Ctx &c, uint32_t d) {
         bool hit = false;
         if (uint32_t(c.lane) < d) {
             const uint32_t mj = c.S->m[c.lane];
-            const uint32_t p = lbound(lst, mdeg, mj);
-            hit = p >= s0 && p < e0 && p < mdeg && __ldg(lst + p) == mj;
+            if ((L.guar_mask >> c.lane) & 1u) {
+                // the query's own arc puts m_j in the list: only the window decides
+                const uint32_t lo = s0 ? __ldg(lst + s0 - 1) : 0;  // window by position
+                hit = (s0 == 0 || mj > lo) && (e0 >= mdeg || mj < __ldg(lst + e0));
+            } else {
+                const uint32_t p = lbound(lst, mdeg, mj);
+                hit = p >= s0 && p < e0 && p < mdeg && __ldg(lst + p) == mj;
+            }
         }
         return (e0 - s0) - __popc(__ballot_sync(kFullMask, hit));
     }
@@ -140,6 +146,44 @@ __device__ unsigned long long count_level(const Ctx &c, uint32_t d) {
         uint32_t v;
         const bool ok = test_candidate(c, d, x0 + c.lane, v);
         n += __popc(__ballot_sync(kFullMask, ok));
+    }
+    return n;
+}
+
+// Level d = k-2 counted together with level k-1 (the plan folded them): each
+// candidate c of level d adds the last level's closed form, the window of the
+// last level's list minus the matched vertices in it, c included.
+__device__ unsigned long long count_level_fold(const Ctx &c, uint32_t d) {
+    const BLevel &F = c.Q->lv[d + 1];
+    const uint32_t s0 = c.S->x[d], e0 = c.S->xend[d];
+    if (s0 >= e0) return 0;
+    const uint32_t u = c.S->m[F.jpos[0]];
+    const uint2 inf = F.jdir[0] ? c.g.in_info[u] : c.g.out_info[u];
+    uint32_t lo = 0, hi = kFullMask;
+    for (uint32_t msk = F.gt_mask; msk; msk &= msk - 1) lo = max(lo, c.S->m[__ffs(msk) - 1] + 1);
+    for (uint32_t msk = F.lt_mask; msk; msk &= msk - 1) hi = min(hi, c.S->m[__ffs(msk) - 1]);
+    const uint32_t *fl = c.g.adj + inf.x;
+    const uint32_t ws = lo ? lbound(fl, inf.y, lo) : 0;
+    const uint32_t we = hi != kFullMask ? lbound(fl, inf.y, hi) : inf.y;
+    bool hit = false;
+    if (uint32_t(c.lane) < d) {
+        const uint32_t mj = c.S->m[c.lane];
+        hit = mj >= lo && mj < hi && (((F.guar_mask >> c.lane) & 1u) || contains(fl, inf.y, mj));
+    }
+    const uint32_t base = (we > ws ? we - ws : 0) - __popc(__ballot_sync(kFullMask, hit));
+    const bool guar_c = (F.guar_mask >> d) & 1u;
+    unsigned long long n = 0;
+    for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
+        uint32_t v;
+        const bool ok = test_candidate(c, d, x0 + c.lane, v);
+        uint32_t add = 0;
+        if (ok) {
+            const bool h2 = v >= lo && v < hi && (guar_c || contains(fl, inf.y, v));
+            add = base - (h2 ? 1u : 0u);
+        }
+        #pragma unroll
+        for (int o = 16; o; o >>= 1) add += __shfl_xor_sync(kFullMask, add, o);
+        n += add;
     }
     return n;
 }
@@ -244,6 +288,10 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
                 qcount += count_level(c, 1);
                 continue;
             }
+            if (Q.k == 3 && Q.lv[1].fold) {
+                qcount += count_level_fold(c, 1);
+                continue;
+            }
             // depth-first over levels 1..k-2, counting level k-1
             uint32_t d = 1;
             bool abandoned = false;
@@ -258,6 +306,7 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
                     __syncwarp();
                     enter_level(c, d + 1);
                     if (d + 2 == Q.k) qcount += count_level(c, d + 1);
+                    else if (d + 3 == Q.k && Q.lv[d + 1].fold) qcount += count_level_fold(c, d + 1);
                     else ++d;
                 } else if (c.S->x[d] < c.S->xend[d]) {
                     if (*vstop || global_ns() > deadline) { abandoned = true; break; }
@@ -370,6 +419,8 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
             B.gt_mask = L.gt_mask;
             B.lt_mask = L.lt_mask;
             B.closed_form = L.closed_form;
+            B.fold = L.fold;
+            B.guar_mask = L.guar_mask;
             for (uint32_t t = 0; t < L.nj; ++t) {
                 B.jpos[t] = L.jpos[t];
                 B.jdir[t] = L.jdir[t];

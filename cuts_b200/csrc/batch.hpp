@@ -13,7 +13,7 @@ constexpr int kBatchMaxJ = 8;   // joined lists per level inside the batched ker
 
 // One level of a batched query (a compact LevelPlan).
 struct BLevel {
-    uint32_t nj, qin, qout, check_sig, gt_mask, lt_mask, closed_form, pad;
+    uint32_t nj, qin, qout, check_sig, gt_mask, lt_mask, closed_form, fold, guar_mask, pad[3];
     uint8_t jpos[kBatchMaxJ];
     uint8_t jdir[kBatchMaxJ];
 };
