@@ -303,7 +303,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuts", choices=["cuts", "reference"])
-    ap.add_argument("--flags", type=int, default=0, help="CUTS_FLAG_* bits")
+    ap.add_argument("--flags", type=int, default=1,
+                    help="CUTS_FLAG_* bits; default 1 = symmetry breaking (exact: one embedding "
+                         "per automorphism orbit, scaled by |Aut(Q)|)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true",
@@ -407,7 +409,7 @@ def main():
         achieved = (ll_bytes / max(ll_n, 1)) / ((ll_ms / max(ll_n, 1)) / 1e3) / 1e9 if ll_ms else None
         traffic = ncu_traffic().get("last_level_bytes_per_launch")
         roofline = {
-            "kernel": "k_level<count> (last trie level)",
+            "kernel": "k_level_flat<count> (last counted trie level)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
             "peak_source": peak_kind,

@@ -1,13 +1,16 @@
-"""Generate tests/golden/ref_counts.json: counts of the reference binary
-(oracle/_ref/cuts_ref, the unmodified reference built for sm_100a by
-`make -C oracle ref`) on this project's seeded inputs.  Runs on a GPU machine:
+"""Generate tests/golden/ref_counts.json: counts of the reference binary built
+for sm_100a by `make -C oracle ref` (oracle/_ref/cuts_ref_b148: the reference
+with its grid set to 148 SMs and its fixed buffers resized so it can start and
+stay in bounds on a B200 host -- the stock build's 280 GB managed reservation
+fails there -- the algorithm untouched) on this project's seeded inputs.
+Runs on a GPU machine:
 
     python tests/golden/make_ref_counts.py
 
 Every input is checked safe for the reference before it runs (SURVEY hazards
 H1/H3): maximum degree below its 15,112-entry per-warp candidate helper, and
 level sizes (from this project's oracle) far below its u32 tables and its
-5e10-word final table.  Each case runs `cuts <data> <query>` and
+(resized) 4e9-word final table.  Each case runs `cuts <data> <query>` and
 `cuts <data> <query> 4`; the fixture records the graph and query recipes
 (not their text) with the counts the reference printed.
 """
@@ -67,9 +70,9 @@ def run_ref(binary, dpath, qpath, trunks=None):
 
 
 def main():
-    binary = O.REF_CUTS
+    binary = O.REF_CUTS.replace("cuts_ref", "cuts_ref_b148")
     assert os.path.exists(binary), "build it: make -C oracle ref"
-    out = {"generator": "tests/golden/make_ref_counts.py", "binary": "oracle/_ref/cuts_ref",
+    out = {"generator": "tests/golden/make_ref_counts.py", "binary": "oracle/_ref/cuts_ref_b148",
            "cases": []}
     with tempfile.TemporaryDirectory() as d:
         for gname, (kind, params) in GRAPHS.items():
@@ -84,8 +87,8 @@ def main():
                 q = cb.Query.from_arcs(k, qarcs)
                 cnt, lv, _ = O.count(od, O.Graph.from_arcs(k, qarcs), q.order)
                 # the reference stores every level of a trunk in one u32 table of
-                # ~3.7e9 words and writes each match into a 5e10-word table
-                if sum(lv[:-1]) > 5e8 or cnt > 5e9:
+                # ~3.6e9 words and writes each match into its final table
+                if sum(lv[:-1]) > 5e8 or cnt > 2e9:
                     continue
                 qpath = os.path.join(d, qname + ".g")
                 cb.write_query(qpath, k, qarcs)

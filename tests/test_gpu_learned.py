@@ -18,9 +18,9 @@ def setup():
     for s in range(80):
         k = 4 + s % 3
         train_q.append((k, cb.random_query_arcs(k, 0.3, 10000 + s)))
-    samples = L.collect(g, train_q, orders_per_query=5, seed=1)
+    samples = L.collect(g, train_q, orders_per_query=8, seed=1)
     X, y, _ = L.features(g, train_q, samples)
-    model = L.train(X, y, epochs=300, batch=1024, lr=2e-3)
+    model = L.train(X, y, epochs=800, batch=1024, lr=2e-3)
     eval_q = []
     for s in range(40):
         k = 4 + s % 3
@@ -44,7 +44,7 @@ def test_learned_order_keeps_counts_and_gains(setup):
         q = cb.Query.from_arcs(k, arcs)
         rs = g.count(q, stats=True)
         ws = L.work(rs.level_sizes, k, L.joins_of(q))
-        order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model)
+        order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, margin=1.5)
         rl = g.count(q, stats=True)
         wl = L.work(rl.level_sizes, k, L.joins_of(q))
         assert rl.count == rs.count
