@@ -94,6 +94,8 @@ _SIGS = {
     "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "cuts_batch_info": (C.c_int, [_vp, _u64p, _u32p]),
     "cuts_batch_free": (None, [_vp]),
+    "cuts_count_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.POINTER(_vp), C.c_uint32,
+                                     C.c_uint32, _vp, _vp]),
     "cuts_mlp_create": (C.c_int, [C.c_uint32, C.c_uint64, C.c_int, C.POINTER(_vp)]),
     "cuts_mlp_param_count": (C.c_int, [_vp, _u32p]),
     "cuts_mlp_get_params": (C.c_int, [_vp, _fp]),
@@ -538,6 +540,17 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def count_noalloc(info_out_ptr: int, info_in_ptr: Optional[int], adj_ptr: int, n: int,
+                  queries: Sequence[Query], counts_ptr: int, flags: int = 0,
+                  stream: Optional[int] = None) -> None:
+    """cuts_count_noalloc: count with caller-owned device buffers only (device
+    addresses as ints, e.g. tensor.data_ptr()).  Asynchronous on `stream`."""
+    nq = len(queries)
+    arr = (_vp * max(nq, 1))(*[q._h for q in queries])
+    _check(lib().cuts_count_noalloc(info_out_ptr, info_in_ptr, adj_ptr, n, arr, nq, flags,
+                                    counts_ptr, stream))
 
 
 def search(query_file: str, data_file: str, write_to_disk: bool = False) -> int:

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -540,6 +541,178 @@ int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int>
         t += r.ms;
     }
     if (ms) *ms = t;
+    return CUTS_OK;
+}
+
+
+// ---- allocation-free entry point ---------------------------------------------
+//
+// For callers that may not allocate GPU memory themselves: code running inside
+// a host framework that owns every device allocation (a memory pool that must
+// account for all bytes, a capture-only execution model, a plugin sandbox).
+// They pass the graph and the output buffer they already own; the engine's
+// own scratch for this path -- the per-query plans and the work counter --
+// lives in the fixed array below, which every GPU that loads this library
+// holds until the process exits.
+namespace {
+
+constexpr uint32_t kNoAllocMaxQueries = 64;  // queries per call
+
+struct NoAllocScratch {
+    BQuery queries[kNoAllocMaxQueries];
+    unsigned long long task_ctr;
+    uint32_t stop;
+    uint32_t aborted[kNoAllocMaxQueries];
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Device address of g_noalloc_scratch per device ordinal (the host-side
+// symbol is only a stand-in, never a device address), and the launch shape.
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocScratch *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+uint32_t g_noalloc_blocks[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Tasks are (query, root vertex) pairs in vertex-id order, query-major; each
+// runs the root's whole level-1 list depth first with the same level steps as
+// k_batch.  No budget: every query runs to completion.
+__global__ void __launch_bounds__(kBW * 32)
+k_batch_noalloc(DevView g, NoAllocScratch *__restrict__ sc, uint32_t nq,
+                unsigned long long *__restrict__ counts) {
+    __shared__ BWarp ws[kBW];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Ctx c{g, nullptr, &ws[warp], lane};
+    const unsigned long long total = (unsigned long long)nq * g.n;
+    uint32_t cur = kFullMask;
+    unsigned long long qcount = 0;
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&sc->task_ctr, 1ull);
+        t = __shfl_sync(kFullMask, t, 0);
+        if (t >= total) break;
+        const uint32_t q = uint32_t(t / g.n), u = uint32_t(t % g.n);
+        if (q != cur) {
+            if (cur != kFullMask && lane == 0 && qcount) atomicAdd(&counts[cur], qcount);
+            qcount = 0;
+            cur = q;
+            c.Q = sc->queries + q;
+        }
+        const BQuery &Q = *c.Q;
+        if (Q.k < 2) continue;
+        const uint2 uo = g.out_info[u], ui = g.in_info[u];
+        if (ui.y < Q.lv[0].qin || uo.y < Q.lv[0].qout) continue;  // level-0 signature
+        if (lane == 0) c.S->m[0] = u;
+        __syncwarp();
+        enter_level(c, 1);  // the whole shortest level-1 list, symmetry window applied
+        if (Q.k == 2) { qcount += count_level(c, 1); continue; }
+        if (Q.k == 3 && Q.lv[1].fold) { qcount += count_level_fold(c, 1); continue; }
+        uint32_t d = 1;
+        while (d >= 1) {
+            if (c.S->bi[d] < c.S->nb[d]) {
+                const uint32_t v = c.S->buf[d][c.S->bi[d]];
+                __syncwarp();
+                if (lane == 0) {
+                    c.S->bi[d]++;
+                    c.S->m[d] = v;
+                }
+                __syncwarp();
+                enter_level(c, d + 1);
+                if (d + 2 == Q.k) qcount += count_level(c, d + 1);
+                else if (d + 3 == Q.k && Q.lv[d + 1].fold) qcount += count_level_fold(c, d + 1);
+                else ++d;
+            } else if (c.S->x[d] < c.S->xend[d]) {
+                refill(c, d);
+            } else {
+                --d;
+            }
+        }
+    }
+    if (cur != kFullMask && lane == 0 && qcount) atomicAdd(&counts[cur], qcount);
+}
+
+}  // namespace
+
+int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint32_t *adj, uint32_t n,
+                  int symmetric, const Query *const *qs, uint32_t nq, uint32_t flags,
+                  unsigned long long *counts, cudaStream_t stream) {
+    if (!info_out || !adj || !counts || (nq && !qs))
+        return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: null argument");
+    if (nq > kNoAllocMaxQueries)
+        return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: more than 64 queries in one call");
+    if (flags & CUTS_FLAG_SYMMETRY_BREAK)
+        return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: symmetry breaking is not available here");
+    // host copy of the query table: on the stack, fixed size, no allocation
+    BQuery table[kNoAllocMaxQueries];
+    const bool sym = symmetric != 0 || info_in == nullptr;
+    for (uint32_t i = 0; i < nq; ++i) {
+        if (!qs[i]) return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: null query");
+        const Query &q = *qs[i];
+        if (q.k > uint32_t(kBatchMaxK))
+            return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: query with more than 10 vertices");
+        Plan plan;
+        int rc = build_plan(q, sym, flags, plan);
+        if (rc) return rc;
+        BQuery &b = table[i];
+        std::memset(&b, 0, sizeof(b));
+        b.k = q.k;
+        for (uint32_t d = 0; d < q.k; ++d) {
+            const LevelPlan &L = plan.lv[d];
+            if (L.nj > uint32_t(kBatchMaxJ))
+                return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: more than 8 joined lists at a level");
+            BLevel &B = b.lv[d];
+            B.nj = L.nj;
+            B.qin = L.qin;
+            B.qout = L.qout;
+            B.check_sig = L.check_sig;
+            B.gt_mask = L.gt_mask;
+            B.lt_mask = L.lt_mask;
+            B.closed_form = L.closed_form;
+            B.fold = L.fold;
+            B.guar_mask = L.guar_mask;
+            for (uint32_t t = 0; t < L.nj; ++t) {
+                B.jpos[t] = L.jpos[t];
+                B.jdir[t] = L.jdir[t];
+            }
+        }
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: no current CUDA device");
+    NoAllocScratch *sc = nullptr;
+    uint32_t blocks = 0;
+    {
+        // once per device, with that device current: the scratch array's
+        // device address and the persistent grid size
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+                return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: cudaGetSymbolAddress failed");
+            int bps = 0, sms = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_noalloc, kBW * 32, 0) != cudaSuccess ||
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+                return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: device query failed");
+            g_noalloc_blocks[dev] = uint32_t(std::max(1, bps) * std::max(1, sms));
+            g_noalloc_ptr[dev] = static_cast<NoAllocScratch *>(p);
+        }
+        sc = g_noalloc_ptr[dev];
+        blocks = g_noalloc_blocks[dev];
+    }
+    // counts and the work counter start at zero on every call
+    if (cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * std::max<uint32_t>(nq, 1), stream) != cudaSuccess ||
+        cudaMemsetAsync(&sc->task_ctr, 0, sizeof(unsigned long long) + sizeof(uint32_t), stream) != cudaSuccess)
+        return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: memset failed");
+    if (nq == 0 || n == 0) return CUTS_OK;
+    if (cudaMemcpyAsync(sc->queries, table, sizeof(BQuery) * nq, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: plan upload failed");
+    const DevView view{reinterpret_cast<const uint2 *>(info_out),
+                       reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n};
+    const unsigned long long total = (unsigned long long)nq * n;
+    const uint32_t grid = uint32_t(std::min<unsigned long long>(blocks, (total + kBW - 1) / kBW));
+    k_batch_noalloc<<<std::max<uint32_t>(grid, 1), kBW * 32, 0, stream>>>(view, sc, nq, counts);
+    if (cudaGetLastError() != cudaSuccess)
+        return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: launch failed");
     return CUTS_OK;
 }
 

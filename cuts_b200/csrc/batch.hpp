@@ -70,4 +70,10 @@ struct Batch {
     int capture(unsigned long long budget_ns);
 };
 
+// The allocation-free count (cuts_count_noalloc): graph and counts in the
+// caller's device memory, engine scratch in a fixed device array.
+int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint32_t *adj, uint32_t n,
+                  int symmetric, const Query *const *qs, uint32_t nq, uint32_t flags,
+                  unsigned long long *counts, cudaStream_t stream);
+
 }  // namespace cuts

@@ -555,4 +555,16 @@ int cuts_count_batch(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t f
     return rc;
 }
 
+int cuts_count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint32_t *adj,
+                       uint32_t n, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                       uint64_t *counts, void *stream) {
+    const Query *ptrs[64];
+    if (nq > 64) return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: more than 64 queries in one call");
+    if (nq && !qs) return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: null query array");
+    for (uint32_t i = 0; i < nq; ++i) ptrs[i] = qs[i] ? &qs[i]->q : nullptr;
+    return count_noalloc(info_out, info_in, adj, n, info_in == nullptr, ptrs, nq, flags,
+                         reinterpret_cast<unsigned long long *>(counts),
+                         static_cast<cudaStream_t>(stream));
+}
+
 }  // extern "C"

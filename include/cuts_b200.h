@@ -256,6 +256,37 @@ int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status
 int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks);
 void cuts_batch_free(cuts_batch b);
 
+/* ---- allocation-free counting ------------------------------------- */
+
+/* For callers that cannot allocate GPU memory themselves -- code inside a
+ * host framework that owns every device allocation (a pool that must
+ * account for all bytes, a sandboxed plugin): count up to 64 queries in one
+ * launch using only buffers the caller passes in.  No reference counterpart.
+ *
+ * Inputs, in the caller's device memory: info_out[2v] = offset of v's sorted
+ * out-list in adj, info_out[2v+1] = its length (u32 pairs, 8-byte aligned);
+ * info_in likewise for in-lists, or NULL for a symmetric graph; adj (u32).
+ * Output: counts[nq] (u64, device memory), overwritten with the exact count
+ * of each query.  Work is queued on `stream` (a cudaStream_t, NULL = the
+ * default stream) and the call returns without waiting; synchronise the
+ * stream before reading counts.
+ *
+ * Calls no cudaMalloc, cudaFree or other allocating routine.  The engine's
+ * own scratch for this path (query plans, work counter) is a fixed array of
+ * about 42 KB in device memory that every GPU loading this library holds
+ * until the process exits.  The first call on a device looks up that
+ * array's device address and the launch shape, with the device current;
+ * make that first call before any stream capture.  Every call shares the
+ * array and clears what must start at zero, so calls that overlap on the
+ * GPU (other streams, other threads) race: serialise them.
+ *
+ * Limits, rejected with CUTS_ERR_LIMIT: more than 64 queries, a query of
+ * more than 10 vertices, a level joining more than 8 lists.
+ * CUTS_FLAG_SYMMETRY_BREAK is rejected (CUTS_ERR_ARG). */
+int cuts_count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint32_t *adj,
+                       uint32_t n, const cuts_query *qs, uint32_t nq, uint32_t flags,
+                       uint64_t *counts, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
