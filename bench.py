@@ -285,9 +285,18 @@ def run_other_workload(args):
         qdefs.append(rq)
         for qname, k, qarcs in qdefs:
             q = cb.Query.from_arcs(k, qarcs)
-            r, done = g.count_budget(q, args.budget_ms, chunks=8, flags=args.flags | cb.FLAG_SYMMETRY_BREAK)
+            fl = args.flags | cb.FLAG_SYMMETRY_BREAK
+            est = None
+            for stride in (1 << 20, 1 << 16, 1 << 12):  # root-stripe estimates, growing
+                rs, ok = g.count_sample(q, 0, stride, budget_ms=10000.0, flags=fl)
+                if not ok:
+                    break
+                est = {"stride": stride, "ms": rs.ms, "est_count": rs.count * stride,
+                       "est_levels": [x * stride for x in rs.level_sizes],
+                       "est_full_s": rs.ms * stride / 1e3}
+            r, done = g.count_budget(q, args.budget_ms, chunks=8, flags=fl)
             res[qname] = {"finished": done, "count": r.count if done else None, "ms": r.ms,
-                          "levels": r.level_sizes if done else None}
+                          "levels": r.level_sizes if done else None, "estimate": est}
         rep["queries"] = res
     print(json.dumps(rep), flush=True)
     return 0

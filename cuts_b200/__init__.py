@@ -89,6 +89,8 @@ _SIGS = {
                                    C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "cuts_count_budget": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_double, _u64p,
                                     C.POINTER(C.c_float), _u64p]),
+    "cuts_count_sample": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                    _u64p, C.POINTER(C.c_float), _u64p]),
     "cuts_batch_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.c_uint32, _u32p,
                                     C.POINTER(_vp)]),
     "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
@@ -397,6 +399,18 @@ class Graph:
         cnt, ms = C.c_uint64(), C.c_float()
         lv = np.zeros(q.k, np.uint64)
         rc = lib().cuts_count_budget(self._h, q._h, chunks, flags, budget_ms, C.byref(cnt),
+                                     C.byref(ms), _ptr(lv, _u64p))
+        if rc == ERR_BUDGET:
+            return CountResult(0, budget_ms, [int(x) for x in lv]), False
+        _check(rc)
+        return CountResult(cnt.value, ms.value, [int(x) for x in lv]), True
+
+    def count_sample(self, q: Query, shard: int, nshards: int, budget_ms: float = 0.0,
+                     flags: int = 0):
+        """(CountResult, finished) of the root stripe u % nshards == shard."""
+        cnt, ms = C.c_uint64(), C.c_float()
+        lv = np.zeros(q.k, np.uint64)
+        rc = lib().cuts_count_sample(self._h, q._h, shard, nshards, flags, budget_ms, C.byref(cnt),
                                      C.byref(ms), _ptr(lv, _u64p))
         if rc == ERR_BUDGET:
             return CountResult(0, budget_ms, [int(x) for x in lv]), False

@@ -354,6 +354,17 @@ int cuts_count_budget(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flag
     return count_impl(g, q, opt, count, ms, level_sizes, nullptr);
 }
 
+int cuts_count_sample(cuts_graph g, cuts_query q, uint32_t shard, uint32_t nshards,
+                      uint32_t flags, double budget_ms, uint64_t *count, float *ms,
+                      uint64_t *level_sizes) {
+    CountOptions opt;
+    opt.flags = flags;
+    opt.shard = shard;
+    opt.nshards = nshards;
+    opt.budget_ms = budget_ms;
+    return count_impl(g, q, opt, count, ms, level_sizes, nullptr);
+}
+
 int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count) {
     if (!g || !g->dev || !q || !path) return set_error(CUTS_ERR_ARG, "null argument");
     GUARD(device_dump(*g->dev, q->q, path, count));

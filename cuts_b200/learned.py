@@ -51,17 +51,21 @@ class Sample:
     score: bool
 
 
-def level_sizes(g: "cb.Graph", q: "cb.Query", stride: int) -> Tuple[List[int], float]:
-    """Per-level sizes of q's current order, from the root stripe 0 of `stride`."""
-    if stride <= 1:
+def level_sizes(g: "cb.Graph", q: "cb.Query", stride: int, budget_ms: float = 0.0):
+    """Per-level sizes of q's current order, from the root stripe 0 of `stride`
+    (scaled by the stride); None when the run exceeds budget_ms."""
+    if stride <= 1 and budget_ms <= 0:
         r = g.count(q, stats=True)
         return r.level_sizes, r.ms
-    r = g.count_sharded(q, 0, stride)
-    return [x * stride for x in r.level_sizes], r.ms
+    r, done = g.count_sample(q, 0, max(stride, 1), budget_ms)
+    if not done:
+        return None, budget_ms
+    return [x * max(stride, 1) for x in r.level_sizes], r.ms
 
 
 def collect(g: "cb.Graph", queries: Sequence[Tuple[int, list]], orders_per_query: int = 4,
-            stride: int = 1, seed: int = 0, time_budget_s: float = 1e9) -> List[Sample]:
+            stride: int = 1, seed: int = 0, time_budget_s: float = 1e9,
+            run_budget_ms: float = 0.0) -> List[Sample]:
     rng = np.random.default_rng(seed)
     out: List[Sample] = []
     t0 = time.time()
@@ -73,7 +77,9 @@ def collect(g: "cb.Graph", queries: Sequence[Tuple[int, list]], orders_per_query
         orders = [score] + [random_order(k, arcs, rng) for _ in range(orders_per_query - 1)]
         for j, o in enumerate(orders):
             q.set_order(o)
-            lv, ms = level_sizes(g, q, stride)
+            lv, ms = level_sizes(g, q, stride, run_budget_ms)
+            if lv is None:  # too expensive to log within the run budget
+                continue
             out.append(Sample(qi, list(o), lv, ms, j == 0))
     return out
 

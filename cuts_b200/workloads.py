@@ -68,12 +68,13 @@ def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0):
     return res, time.perf_counter() - t0
 
 
-def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 256,
-                epochs: int = 300, seed: int = 10000, time_budget_s: float = 600.0):
+def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1024,
+                epochs: int = 400, seed: int = 10000, time_budget_s: float = 300.0,
+                run_budget_ms: float = 100.0):
     train_q = eval_queries(n_train, seed0=seed)
     t0 = time.perf_counter()
     samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
-                        time_budget_s=time_budget_s)
+                        time_budget_s=time_budget_s, run_budget_ms=run_budget_ms)
     t_collect = time.perf_counter() - t0
     X, y, _ = L.features(g, train_q, samples)
     t1 = time.perf_counter()
@@ -94,16 +95,23 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
     qdefs = eval_queries(n_eval)
     plain, plain_s = plain_pass(g, qdefs, budget_ms, flags)
     t0 = time.perf_counter()
-    qs = []
+    qs, works = [], []
     switched = 0
     for k, arcs in qdefs:
         q = cb.Query.from_arcs(k, arcs)
-        _, pw, sw = q.plan(g, cb.ORDER_LEARNED, model)
+        _, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, beam=256)
         switched += pw < sw
         qs.append(q)
+        works.append(pw)
+    # cheapest predicted work first, so the launch budget cuts only the costliest
+    rank = sorted(range(n_eval), key=lambda i: works[i])
     plan_s = time.perf_counter() - t0
-    b = g.batch(qs, flags=flags)
-    counts, status, ms = b.run(budget_ms * n_eval)
+    b = g.batch([qs[i] for i in rank], flags=flags)
+    counts_r, status_r, ms = b.run(budget_ms * n_eval)
+    counts = [0] * n_eval
+    status = [0] * n_eval
+    for j, i in enumerate(rank):
+        counts[i], status[i] = counts_r[j], status_r[j]
     learned_s = plan_s + ms / 1e3
     done_p = [d for d, _, _ in plain]
     done_l = [s == 0 for s in status]

@@ -184,6 +184,13 @@ int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t fla
 int cuts_count_budget(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
                       double budget_ms, uint64_t *count, float *ms, uint64_t *level_sizes);
 
+/* The root stripe u % nshards == shard of cuts_count, under a time budget
+ * (0 = none): the per-level sizes of a stripe, scaled by nshards, estimate the
+ * full run's.  Used to log training data for the learned order cheaply. */
+int cuts_count_sample(cuts_graph g, cuts_query q, uint32_t shard, uint32_t nshards,
+                      uint32_t flags, double budget_ms, uint64_t *count, float *ms,
+                      uint64_t *level_sizes);
+
 /* Write every embedding to `path` in the reference's ans.txt line format
  * "(q,d)(q,d)..." in matching order (util.cpp:53-74).  Returns the number
  * of lines in *count.  Line order is unspecified, as in the reference. */
