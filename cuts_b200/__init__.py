@@ -32,6 +32,7 @@ ERR_ARG, ERR_IO, ERR_PARSE, ERR_CUDA, ERR_NOMEM, ERR_QUERY, ERR_CAPACITY, ERR_LI
 MAX_QUERY = 16
 FLAG_SYMMETRY_BREAK = 1
 FLAG_NO_CLOSED_FORM = 2
+FLAG_NO_FUSE = 4
 ORDER_SCORE = 0
 ORDER_LEARNED = 1
 
@@ -295,8 +296,8 @@ class Query:
         aut = C.c_uint64()
         _check(lib().cuts_query_plan_levels(self._h, int(data_symmetric), flags, _ptr(out, _u32p),
                                             C.byref(aut)))
-        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt"]
-        return [dict(zip(keys, (int(x) for x in out[8 * i:8 * i + 7]))) for i in range(k)], aut.value
+        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse"]
+        return [dict(zip(keys, (int(x) for x in out[8 * i:8 * i + 8]))) for i in range(k)], aut.value
 
     def automorphisms(self) -> int:
         a = C.c_uint64()

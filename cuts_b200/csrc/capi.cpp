@@ -278,7 +278,7 @@ int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uin
             const LevelPlan &L = p.lv[i];
             uint32_t *o = out + 8 * i;
             o[0] = L.nj; o[1] = L.check_sig; o[2] = L.closed_form; o[3] = L.fold;
-            o[4] = L.guar_mask; o[5] = L.gt_mask; o[6] = L.lt_mask; o[7] = 0;
+            o[4] = L.guar_mask; o[5] = L.gt_mask; o[6] = L.lt_mask; o[7] = L.fuse;
         }
         if (aut) *aut = p.aut;
         return CUTS_OK;

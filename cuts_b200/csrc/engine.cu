@@ -56,7 +56,8 @@ constexpr uint32_t kTile = 256; // planner tile (parents)
 struct RunParams {
     Plan plan;
     uint32_t stored;   // levels kept in HBM: k-1 when counting, k when dumping
-    uint32_t pad_[3];
+    uint32_t fuse_stride;  // words per warp row of the fused kernel's scratch
+    uint32_t *fuse_scratch;
     uint32_t *vert[kMaxK];
     uint32_t *par[kMaxK];
     uint32_t *ub[kMaxK];
@@ -608,6 +609,265 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     }
 }
 
+// ---- fused count of levels p and c = p + 1 ---------------------------
+// When the plan fuses the counted level c with p = c - 1, c's candidates for
+// a vertex s chosen at p are the members t of p's candidate set S (same
+// parent) that lie in s's list.  One warp per parent at level p - 1: build S
+// once (the usual scan of the shortest joined list, membership in the
+// others, ballot compaction) into the warp's scratch row, then for every s
+// in S intersect S with s's list -- iterating whichever of the two is
+// shorter, lane-parallel, with lower-bound probes into the other -- and
+// count (or, for a folded c, add the last level's closed form per t).  Level
+// p is never written to the trie.
+constexpr int kZW = 4;  // warps per block
+
+template <int MODE>
+__global__ void __launch_bounds__(kZW * 32)
+k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb,
+        uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride,
+        unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,
+        unsigned long long *__restrict__ acc_p) {
+    __shared__ LevelPlan sP, sC, sF;
+    __shared__ uint32_t *s_vert[kMaxK];
+    __shared__ uint32_t *s_par[kMaxK];
+    __shared__ uint32_t s_k;
+    __shared__ uint32_t wm[kZW][kMaxK];
+    __shared__ uint32_t joff[kZW][kMaxJ], jdeg[kZW][kMaxJ];
+    __shared__ uint32_t xoff[kZW][kMaxJ], xdeg[kZW][kMaxJ];
+    {
+        const uint32_t words = sizeof(LevelPlan) / 4;
+        const uint32_t c = p + 1;
+        const uint32_t f = c + 1 < rp->plan.k ? c + 1 : c;
+        const uint32_t *a = reinterpret_cast<const uint32_t *>(&rp->plan.lv[p]);
+        const uint32_t *b = reinterpret_cast<const uint32_t *>(&rp->plan.lv[c]);
+        const uint32_t *d = reinterpret_cast<const uint32_t *>(&rp->plan.lv[f]);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+            reinterpret_cast<uint32_t *>(&sP)[i] = a[i];
+            reinterpret_cast<uint32_t *>(&sC)[i] = b[i];
+            reinterpret_cast<uint32_t *>(&sF)[i] = d[i];
+        }
+        if (threadIdx.x < kMaxK) {
+            s_vert[threadIdx.x] = rp->vert[threadIdx.x];
+            s_par[threadIdx.x] = rp->par[threadIdx.x];
+        }
+        if (threadIdx.x == 0) s_k = rp->plan.k;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lanemask_lt = (1u << lane) - 1;
+    uint32_t *my_m = wm[warp];
+    uint32_t *S = scratch + size_t(blockIdx.x * kZW + warp) * stride;
+    const uint32_t c = p + 1;
+    // the counted level c is folded when level c carries the fold flag
+    const bool cfold = sC.fold != 0;
+    const uint32_t tp = sC.fuse_tp;
+    const uint32_t extra = sC.fuse_extra;
+    const bool sig_c = sC.check_sig && (sC.qin > sP.qin || sC.qout > sP.qout);
+    const uint32_t below = (1u << p) - 1;
+    const bool c_gt_s = (sC.gt_mask >> p) & 1u, c_lt_s = (sC.lt_mask >> p) & 1u;
+    const bool fguar_t = cfold && ((sF.guar_mask >> c) & 1u);
+    unsigned long long local = 0, local_c = 0, local_p = 0;
+    uint32_t cached_q = kFullMask;
+    const uint32_t total = pb - pa;
+    auto probes = [](uint32_t len) { return 32u - __clz(len | 1u); };
+
+    while (true) {
+        uint32_t gi = 0;
+        if (lane == 0) gi = atomicAdd(cursor, 1u);
+        gi = __shfl_sync(kFullMask, gi, 0);
+        if (gi >= total) break;
+        const uint32_t q0 = pa + gi;
+        if (lane == 0) {  // matched vertices of the parent at level p-1
+            my_m[p - 1] = s_vert[p - 1][q0];
+            if (p >= 2) {
+                uint32_t q = s_par[p - 1][q0];
+                if (q != cached_q) {
+                    cached_q = q;
+                    for (int j = int(p) - 2; j >= 0; --j) {
+                        my_m[j] = s_vert[j][q];
+                        if (j > 0) q = s_par[j][q];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // level p: joined lists, the shortest supplies S
+        const uint32_t njp = sP.nj;
+        uint32_t md = kFullMask, mo = 0;
+        if (uint32_t(lane) < njp) {
+            const uint32_t u = my_m[sP.jpos[lane]];
+            const uint2 inf = sP.jdir[lane] ? g.in_info[u] : g.out_info[u];
+            mo = inf.x;
+            md = inf.y;
+            joff[warp][lane] = mo;
+            jdeg[warp][lane] = md;
+        }
+        uint32_t bd = md, bl = uint32_t(lane);
+        #pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const uint32_t od = __shfl_xor_sync(kFullMask, bd, o), ol = __shfl_xor_sync(kFullMask, bl, o);
+            if (od < bd || (od == bd && ol < bl)) { bd = od; bl = ol; }
+        }
+        const uint32_t moff = __shfl_sync(kFullMask, mo, int(bl)), mdeg = njp ? bd : 0, tmin = bl;
+        // extra lists of level c on positions below p: fixed for this parent
+        if (uint32_t(lane) < sC.nj && ((extra >> lane) & 1u) && sC.jpos[lane] < p) {
+            const uint32_t u = my_m[sC.jpos[lane]];
+            const uint2 inf = sC.jdir[lane] ? g.in_info[u] : g.out_info[u];
+            xoff[warp][lane] = inf.x;
+            xdeg[warp][lane] = inf.y;
+        }
+        __syncwarp();
+        uint32_t lo = 0, hi = kFullMask;
+        for (uint32_t msk = sP.gt_mask; msk; msk &= msk - 1) lo = max(lo, my_m[__ffs(msk) - 1] + 1);
+        for (uint32_t msk = sP.lt_mask; msk; msk &= msk - 1) hi = min(hi, my_m[__ffs(msk) - 1]);
+        const uint32_t *mlist = g.adj + moff;
+        const uint32_t s0 = lo ? lbound(mlist, mdeg, lo) : 0;
+        const uint32_t e0 = hi != kFullMask ? lbound(mlist, mdeg, hi) : mdeg;
+        uint32_t ns = 0;
+        for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
+            const uint32_t x = x0 + lane;
+            bool ok = x < e0;
+            const uint32_t v = ok ? __ldg(mlist + x) : 0;
+            if (ok)
+                for (uint32_t j = 0; j < p; ++j)
+                    if (v == my_m[j]) { ok = false; break; }
+            if (ok) {
+                const uint2 o = g.out_info[v], i = g.in_info[v];
+                ok = i.y >= sP.qin && o.y >= sP.qout;
+            }
+            if (ok)
+                for (uint32_t t = 0; t < njp; ++t) {
+                    if (t == tmin) continue;
+                    if (!contains(g.adj + joff[warp][t], jdeg[warp][t], v)) { ok = false; break; }
+                }
+            const unsigned m = __ballot_sync(kFullMask, ok);
+            if (ok) S[ns + __popc(m & lanemask_lt)] = v;
+            ns += __popc(m);
+            if (MODE == kBytesMode && lane == 0) {
+                uint32_t per = 8;
+                for (uint32_t t = 0; t < njp; ++t)
+                    if (t != tmin) per += 4 * probes(jdeg[warp][t]);
+                local += 4ull * min(32u, e0 - x0) + uint64_t(min(32u, e0 - x0)) * per;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            local_p += ns;
+            if (MODE == kBytesMode) local += 8ull * p + 8ull * njp + 4ull * ns;
+        }
+        // level c over the vertices s of S
+        uint32_t lo_c = 0, hi_c = kFullMask;
+        for (uint32_t msk = sC.gt_mask & below; msk; msk &= msk - 1) lo_c = max(lo_c, my_m[__ffs(msk) - 1] + 1);
+        for (uint32_t msk = sC.lt_mask & below; msk; msk &= msk - 1) hi_c = min(hi_c, my_m[__ffs(msk) - 1]);
+        for (uint32_t i = 0; i < ns; ++i) {
+            const uint32_t sv = S[i];
+            const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
+            const uint32_t *Ls = g.adj + is.x;
+            const uint32_t ds = is.y;
+            uint32_t lo_t = lo_c, hi_t = hi_c;
+            if (c_gt_s) lo_t = max(lo_t, sv + 1);
+            if (c_lt_s) hi_t = min(hi_t, sv);
+            const uint32_t ts = lo_t ? lbound(S, ns, lo_t) : 0;
+            const uint32_t te = hi_t != kFullMask ? lbound(S, ns, hi_t) : ns;
+            if (ts >= te) continue;
+            // per-s extra lists of level c (joins on p in the other direction)
+            if (uint32_t(lane) < sC.nj && ((extra >> lane) & 1u) && sC.jpos[lane] == p) {
+                const uint2 inf = sC.jdir[lane] ? g.in_info[sv] : g.out_info[sv];
+                xoff[warp][lane] = inf.x;
+                xdeg[warp][lane] = inf.y;
+            }
+            // folded last level: f_base(s) = |window of L_F| - matched in it
+            uint32_t fbase = 0, fdeg = 0, flo = 0, fhi = kFullMask;
+            const uint32_t *fl = nullptr;
+            if (cfold) {
+                const uint32_t jf = sF.jpos[0];
+                const uint32_t u = jf == p ? sv : my_m[jf];
+                const uint2 inf = sF.jdir[0] ? g.in_info[u] : g.out_info[u];
+                fl = g.adj + inf.x;
+                fdeg = inf.y;
+                for (uint32_t msk = sF.gt_mask; msk; msk &= msk - 1) {
+                    const uint32_t j = __ffs(msk) - 1;
+                    flo = max(flo, (j == p ? sv : my_m[j]) + 1);
+                }
+                for (uint32_t msk = sF.lt_mask; msk; msk &= msk - 1) {
+                    const uint32_t j = __ffs(msk) - 1;
+                    fhi = min(fhi, j == p ? sv : my_m[j]);
+                }
+                const uint32_t ws = flo ? lbound(fl, fdeg, flo) : 0;
+                const uint32_t we = fhi != kFullMask ? lbound(fl, fdeg, fhi) : fdeg;
+                bool hit = false;
+                if (uint32_t(lane) <= p) {
+                    const uint32_t mj = uint32_t(lane) == p ? sv : my_m[lane];
+                    hit = mj >= flo && mj < fhi && (((sF.guar_mask >> lane) & 1u) || contains(fl, fdeg, mj));
+                }
+                fbase = (we > ws ? we - ws : 0) - __popc(__ballot_sync(kFullMask, hit));
+            }
+            __syncwarp();
+            const uint32_t ls0 = lo_t ? lbound(Ls, ds, lo_t) : 0;
+            const uint32_t ls1 = hi_t != kFullMask ? lbound(Ls, ds, hi_t) : ds;
+            const uint32_t nS = te - ts, nL = ls1 > ls0 ? ls1 - ls0 : 0;
+            const bool iterS = nS <= nL;
+            const uint32_t nit = iterS ? nS : nL;
+            if (MODE == kBytesMode) {
+                if (lane == 0)
+                    local += 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iterS ? ds : nS) +
+                             (sig_c ? 8ull * nit : 0) + (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
+                continue;
+            }
+            uint32_t gal = iterS ? ls0 : ts;
+            for (uint32_t y0 = 0; y0 < nit; y0 += 32) {
+                const uint32_t y = y0 + lane;
+                bool ok = y < nit;
+                uint32_t t = 0;
+                if (ok) {
+                    if (iterS) {
+                        t = S[ts + y];
+                        const uint32_t pos = lbound_from(Ls, ls1, gal, t);
+                        gal = pos;
+                        ok = pos < ls1 && __ldg(Ls + pos) == t;
+                    } else {
+                        t = __ldg(Ls + ls0 + y);
+                        const uint32_t pos = lbound_from(S, te, gal, t);
+                        gal = pos;
+                        ok = pos < te && S[pos] == t;
+                    }
+                }
+                if (ok && t == sv) ok = false;
+                if (ok && extra)
+                    for (uint32_t tt = 0; tt < sC.nj; ++tt)
+                        if ((extra >> tt) & 1u)
+                            if (!contains(g.adj + xoff[warp][tt], xdeg[warp][tt], t)) { ok = false; break; }
+                if (ok && sig_c) {
+                    const uint2 o = g.out_info[t], i2 = g.in_info[t];
+                    ok = i2.y >= sC.qin && o.y >= sC.qout;
+                }
+                if (ok) {
+                    ++local_c;
+                    if (cfold) {
+                        const bool h = t >= flo && t < fhi && (fguar_t || contains(fl, fdeg, t));
+                        local += fbase - (h ? 1u : 0u);
+                    } else {
+                        ++local;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    #pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        local += __shfl_xor_sync(kFullMask, local, o);
+        local_c += __shfl_xor_sync(kFullMask, local_c, o);
+    }
+    if (lane == 0) {
+        if (local) atomicAdd(acc, local);
+        if (MODE == kCountMode) {
+            if (local_c) atomicAdd(acc_c, local_c);
+            if (local_p) atomicAdd(acc_p, local_p);
+        }
+    }
+}
+
 // ---- chunk planner ------------------------------------------------------
 // Tile sums of the child bounds of parents [pa, pb).
 __global__ void k_tile_sums(const uint32_t *__restrict__ ub, uint32_t pa, uint32_t pb,
@@ -705,6 +965,7 @@ k_plan(const uint64_t *__restrict__ tsum, uint32_t ntiles, unsigned long long ca
 int g_num_sms = 0;
 int g_level_blocks[3] = {0, 0, 0};
 int g_flat_blocks[3] = {0, 0, 0};
+int g_fused_blocks[3] = {0, 0, 0};
 // CUTS_LEVEL_KERNEL=warp selects the warp-per-parent form (A/B comparisons)
 bool g_use_flat = true;
 
@@ -726,6 +987,10 @@ int launch_geometry() {
     g_flat_blocks[kCountMode] = std::max(1, b) * g_num_sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level_flat<kBytesMode>, kFW * 32, 0));
     g_flat_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kCountMode>, kZW * 32, 0));
+    g_fused_blocks[kCountMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kBytesMode>, kZW * 32, 0));
+    g_fused_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
     const char *kv = std::getenv("CUTS_LEVEL_KERNEL");
     g_use_flat = !(kv && std::strcmp(kv, "warp") == 0);
     return CUTS_OK;
@@ -975,6 +1240,32 @@ struct Run {
         return CUTS_OK;
     }
 
+    // The fused count of levels p and p+1 over parents [pa, pb) of L_{p-1}.
+    int launch_fused(int mode, uint32_t p, uint32_t pa, uint32_t pb) {
+        CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
+        const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_blocks[mode]),
+                                                                         (pb - pa + kZW - 1) / kZW));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (profile) {
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            CK(cudaEventRecord(e0, g.stream));
+        }
+        if (mode == kBytesMode)
+            k_fused<kBytesMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, g.d_u32 + kSlotCursor,
+                hp->fuse_scratch, hp->fuse_stride, g.d_u64 + 2, nullptr, nullptr);
+        else
+            k_fused<kCountMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, g.d_u32 + kSlotCursor,
+                hp->fuse_scratch, hp->fuse_stride, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
+        CK(cudaGetLastError());
+        if (profile) {
+            CK(cudaEventRecord(e1, g.stream));
+            marks.push_back({kCountMode, {e0, e1}});
+        }
+        res.launches++;
+        return CUTS_OK;
+    }
+
     // Sums the profiled launch times per kernel (after a sync).
     void collect_profile() {
         for (auto &m : marks) {
@@ -991,8 +1282,11 @@ struct Run {
     // Expands parents [pa, pb) of L_{lvl-1}, depth first by chunks.
     int expand(uint32_t lvl, uint32_t pa, uint32_t pb) {
         if (pb <= pa) return CUTS_OK;
-        // the last level is counted; with a folded plan, level k-2 counts both
+        // the last level is counted; with a folded plan, level k-2 counts both;
+        // with a fused plan, the counting kernel runs one level earlier
         const uint32_t count_lvl = (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
+        if (!dump && k >= 3 && hp->plan.lv[count_lvl].fuse && lvl == count_lvl - 1)
+            return launch_fused(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
         if (lvl == count_lvl && !dump) {
             int rc = launch_level(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
             return rc;
@@ -1061,11 +1355,22 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     std::memset(hp, 0, sizeof(RunParams));
     int rc = build_plan(q, g.symmetric, flags, hp->plan);
     if (rc) return rc;
+    const bool counting = stored == k - 1;
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
-        // the folded count runs in the flattened kernel only
-        if (!g_use_flat || hp->plan.lv[k - 2].nj > uint32_t(kFJ)) hp->plan.lv[k - 2].fold = 0;
-        else if (stored == k - 1) stored = k - 2;  // level k-2 is counted, not stored
+        // the folded count runs in the flattened or the fused kernel only
+        const bool fused_here = hp->plan.lv[k - 2].fuse != 0;
+        if (!fused_here && (!g_use_flat || hp->plan.lv[k - 2].nj > uint32_t(kFJ))) hp->plan.lv[k - 2].fold = 0;
+        else if (counting) stored = k - 2;  // level k-2 is counted, not stored
     }
+    // the counted level and, when fused, the one before it are not stored
+    const uint32_t cl = (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
+    if (k >= 3 && !hp->plan.lv[k - 2].fold) hp->plan.lv[k - 2].fuse = 0;
+    // CUTS_NO_FUSE=1 turns fusion off process-wide (A/B comparisons)
+    const char *nf = std::getenv("CUTS_NO_FUSE");
+    if (!counting || (nf && nf[0] == '1'))
+        for (uint32_t i = 0; i < k; ++i) hp->plan.lv[i].fuse = 0;
+    const bool fuse = counting && k >= 3 && hp->plan.lv[cl].fuse;
+    if (fuse) stored = cl - 1;
     hp->stored = stored;
     if (!g.arena) {
         cudaError_t e = cudaMalloc(&g.arena, g.arena_bytes);
@@ -1077,10 +1382,20 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     // L_0: vert + ub (n entries each); L_1..L_{stored-1}: vert + par + ub
     const uint64_t n = g.n;
     const uint64_t l0_bytes = ((8 * n + 255) / 256) * 256 + 256;
+    // fused kernel: one scratch row per resident warp, as long as the longest list
+    uint64_t fuse_bytes = 0;
+    if (fuse) {
+        hp->fuse_stride = ((std::max<uint32_t>(g.max_deg, 1) + 31) / 32) * 32;
+        fuse_bytes = uint64_t(g_fused_blocks[kCountMode] > g_fused_blocks[kBytesMode] ? g_fused_blocks[kCountMode]
+                                                                                      : g_fused_blocks[kBytesMode]) *
+                     kZW * hp->fuse_stride * 4;
+    }
     cap = 0;
-    if (g.arena_bytes < l0_bytes) return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level");
+    if (g.arena_bytes < l0_bytes + fuse_bytes)
+        return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level and scratch");
+    if (fuse) hp->fuse_scratch = reinterpret_cast<uint32_t *>(static_cast<char *>(g.arena) + g.arena_bytes - fuse_bytes);
     if (stored >= 2) {
-        cap = (g.arena_bytes - l0_bytes) / (12ull * (stored - 1));
+        cap = (g.arena_bytes - l0_bytes - fuse_bytes) / (12ull * (stored - 1));
         cap = std::min<uint64_t>(cap, (1ull << 31) - 64);
         if (g.level_cap_req) cap = std::min<uint64_t>(cap, g.level_cap_req);
         cap &= ~uint64_t(63);
@@ -1215,6 +1530,13 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
         CK(cudaMemcpy(g.h_u64 + 3, g.d_u64 + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         res.level_sizes[k - 2] = g.h_u64[3];
+    }
+    if (k >= 3) {
+        const uint32_t cl = hp->plan.lv[k - 2].fold ? k - 2 : k - 1;
+        if (hp->plan.lv[cl].fuse) {  // the fused level before the counted one
+            CK(cudaMemcpy(g.h_u64 + 4, g.d_u64 + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+            res.level_sizes[cl - 1] = g.h_u64[4];
+        }
     }
     res.count = raw * hp->plan.aut;
     if (opt.want_bytes && k >= 2 && n0 > 0) {

@@ -95,7 +95,10 @@ struct LevelPlan {
                               // independent of this level's vertex)
     uint32_t guar_mask;       // last level: positions whose vertex the query's
                               // own arcs guarantee to be in the joined list
-    uint32_t pad2[3];
+    uint32_t fuse;            // counted level c: count it from level c-1's
+                              // candidate sets (see build_plan)
+    uint32_t fuse_extra;      // mask of c's joins beyond c-1's joins and (c-1)
+    uint32_t fuse_tp;         // index of c's join on position c-1
     uint8_t jpos[kMaxJ];      // joined position j
     uint8_t jdir[kMaxJ];      // 0: out-list of m_j (P join), 1: in-list (C join)
 };

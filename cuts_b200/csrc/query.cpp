@@ -316,6 +316,36 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
         const uint32_t pen = 1u << (k - 2);
         if (F.jpos[0] != k - 2 && !(F.gt_mask & pen) && !(F.lt_mask & pen)) plan.lv[k - 2].fold = 1;
     }
+    // Fuse the counted level c with level p = c-1 when c's candidates are a
+    // subset of p's: every list p joins is joined at c too, c also joins p's
+    // own vertex, p's signature is no stricter than c's, and p's symmetry
+    // window is no narrower than c's (p's conditions are among c's).  Then,
+    // for one parent at level p-1, p's candidate set S serves every vertex s
+    // chosen at p: c's candidates are the t in S that lie in s's list.
+    if (k >= 3 && !(flags & CUTS_FLAG_NO_FUSE)) {
+        const uint32_t c = (plan.lv[k - 2].fold) ? k - 2 : k - 1;
+        const uint32_t p = c - 1;
+        LevelPlan &Lc = plan.lv[c];
+        const LevelPlan &Lp = plan.lv[p];
+        bool ok = p >= 1 && !Lc.closed_form && Lp.check_sig && Lc.qin >= Lp.qin && Lc.qout >= Lp.qout;
+        const uint32_t below = (1u << p) - 1;
+        ok = ok && (Lp.gt_mask & below & ~Lc.gt_mask) == 0 && (Lp.lt_mask & below & ~Lc.lt_mask) == 0;
+        uint32_t tp = kMaxJ, covered = 0;
+        for (uint32_t t = 0; ok && t < Lc.nj; ++t)
+            if (Lc.jpos[t] == p && tp == kMaxJ) { tp = t; covered |= 1u << t; }
+        ok = ok && tp != kMaxJ;
+        for (uint32_t u = 0; ok && u < Lp.nj; ++u) {
+            bool found = false;
+            for (uint32_t t = 0; t < Lc.nj; ++t)
+                if (Lc.jpos[t] == Lp.jpos[u] && Lc.jdir[t] == Lp.jdir[u]) { found = true; covered |= 1u << t; }
+            ok = found;
+        }
+        if (ok) {
+            Lc.fuse = 1;
+            Lc.fuse_tp = tp;
+            Lc.fuse_extra = ((Lc.nj >= 32) ? ~0u : ((1u << Lc.nj) - 1)) & ~covered;
+        }
+    }
     return CUTS_OK;
 }
 

@@ -35,6 +35,8 @@ extern "C" {
                                         query must be loop-free) */
 #define CUTS_FLAG_NO_CLOSED_FORM 2u  /* enumerate the last level even when a
                                         closed form exists */
+#define CUTS_FLAG_NO_FUSE 4u         /* materialise the level before the counted
+                                        one even when it could be fused */
 
 /* order modes for cuts_plan */
 #define CUTS_ORDER_SCORE 0    /* greedy score order (score.cpp) */
@@ -135,7 +137,8 @@ int cuts_query_set_order(cuts_query q, const uint32_t *order);
 /* The per-level plan the kernels run for the current order, for a data
  * graph that is symmetric or not and the given flags: 8 words per level,
  * {joined lists, signature test, closed form, folded into the level before,
- * guaranteed-member mask, greater-than mask, less-than mask, 0}.  Host only;
+ * guaranteed-member mask, greater-than mask, less-than mask, fused with the
+ * level before}.  Host only;
  * no reference counterpart (the reference derives joins per launch,
  * device_funcs.cu:103-127). */
 int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,

@@ -245,3 +245,51 @@ def test_fold_and_guaranteed_members(er2k, cl5k, name, flags):
             assert r.level_sizes == lv
         r4 = g.count(q, flags=flags, chunks=3)
         assert r4.count == cnt
+
+
+FUSE_QUERIES = {
+    "triangle": cb.named_query_arcs("triangle"),
+    "4-clique": (4, [(a, b) for a in range(4) for b in range(4) if a != b]),
+    "5-clique": (5, [(a, b) for a in range(5) for b in range(5) if a != b]),
+    "4-clique+pendant": cb.named_query_arcs("4-clique+pendant"),
+    "diamond": (4, [(0, 1), (1, 0), (0, 2), (2, 0), (1, 2), (2, 1), (1, 3), (3, 1), (2, 3), (3, 2)]),
+    "house": cb.named_query_arcs("house"),
+    "directed-triangle-mixed": (3, [(0, 1), (1, 2), (0, 2), (2, 0)]),
+    "directed-4-clique": (4, [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (3, 1)]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FUSE_QUERIES))
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK])
+def test_fused_levels(er2k, cl5k, name, flags):
+    """The counted level fused with the one before (per-parent candidate sets
+    in scratch) against the oracle, levels included, and against the unfused
+    plan; directed queries on a directed graph too."""
+    k, arcs = FUSE_QUERIES[name]
+    graphs = [er2k, cl5k]
+    if name.startswith("directed"):
+        n, src, dst = directed_er(1500, 14.0, seed=11)
+        oo, oa, io, ia, s_, d_ = csr_from_arcs(n, src, dst)
+        graphs = [(None, cb.Graph.from_csr(n, oo, oa, io, ia), O.Graph.from_arrays(n, s_, d_))]
+    for h, g, od in graphs:
+        q = cb.Query.from_arcs(k, arcs)
+        cnt, lv, _ = oracle_count(od, k, arcs, q.order)
+        r = g.count(q, flags=flags, stats=True)
+        assert r.count == cnt
+        if flags == 0:
+            assert r.level_sizes == lv
+        assert g.count(q, flags=flags | cb.FLAG_NO_FUSE).count == cnt
+        assert g.count(q, flags=flags, chunks=5).count == cnt
+
+
+def test_fused_with_forced_chunking(cl5k):
+    h, g, od = cl5k
+    k, arcs = cb.named_query_arcs("4-clique+pendant")
+    q = cb.Query.from_arcs(k, arcs)
+    cnt, lv, _ = oracle_count(od, k, arcs, q.order)
+    g.set_level_cap(2048)
+    try:
+        r = g.count(q, stats=True)
+        assert r.count == cnt and r.level_sizes == lv
+    finally:
+        g.set_level_cap(0)

@@ -203,3 +203,17 @@ def test_plan_directed_guarantees():
     assert lv[3]["guar"] == 0b010
     lv_sym, _ = q.plan_levels(True, 0)
     assert lv_sym[3]["guar"] == 0b010  # 2 is not adjacent to 0 at all
+
+
+def test_plan_fuse_conditions():
+    tri = cb.Query.from_arcs(*cb.named_query_arcs("triangle"))
+    lv, _ = tri.plan_levels(True, 0)
+    assert lv[2]["fuse"] == 1
+    assert tri.plan_levels(True, cb.FLAG_NO_FUSE)[0][2]["fuse"] == 0
+    # 4-clique+pendant: the folded level k-2 (the 4-clique vertex) is fused
+    cp = cb.Query.from_arcs(*cb.named_query_arcs("4-clique+pendant"))
+    lv, _ = cp.plan_levels(True, 0)
+    assert lv[3]["fold"] == 1 and lv[3]["fuse"] == 1
+    # 4-cycle: the last vertex does not join the previous one's lists -> no fuse
+    c4 = cb.Query.from_arcs(*cb.named_query_arcs("4-cycle"))
+    assert all(l["fuse"] == 0 for l in c4.plan_levels(True, 0)[0])
