@@ -161,7 +161,7 @@ def cpu_sample(h, queries, budget_s=20.0):
         n0 = h.n
         # grow a contiguous root slice (vertex-id order; weights are i.i.d. per
         # vertex, so a slice is an unbiased sample) until it takes per_q / 4
-        span = 64
+        span = 8
         while True:
             t0 = time.perf_counter()
             cnt, lv, _ = O.count(od, oq, order, 0, span, cores)
