@@ -62,6 +62,8 @@ _SIGS = {
     "cuts_hgraph_csr": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cuts_hgraph_write": (C.c_int, [_vp, C.c_char_p]),
     "cuts_graph_upload": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "cuts_hgraph_save_binary": (C.c_int, [_vp, C.c_char_p]),
+    "cuts_hgraph_load_binary": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
     "cuts_hgraph_free": (None, [_vp]),
     "cuts_gen_random_query": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _u32p, _u32p, _u32p]),
     "cuts_graph_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
@@ -189,6 +191,15 @@ class HostGraph:
 
     def write(self, path: str) -> None:
         _check(lib().cuts_hgraph_write(self._h, path.encode()))
+
+    def save_binary(self, path: str) -> None:
+        _check(lib().cuts_hgraph_save_binary(self._h, path.encode()))
+
+    @classmethod
+    def load_binary(cls, path: str) -> "HostGraph":
+        h = _vp()
+        _check(lib().cuts_hgraph_load_binary(path.encode(), C.byref(h)))
+        return cls(h)
 
     def upload(self, device: int = 0) -> "Graph":
         g = _vp()

@@ -114,6 +114,23 @@ int cuts_hgraph_write(cuts_hgraph h, const char *path) {
     GUARD(write_graph_text(path, h->g));
 }
 
+int cuts_hgraph_save_binary(cuts_hgraph h, const char *path) {
+    if (!h || !path) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(save_graph_binary(path, h->g));
+}
+
+int cuts_hgraph_load_binary(const char *path, cuts_hgraph *out) {
+    if (!path || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_hgraph_s>();
+        int rc = load_graph_binary(path, h->g);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
 int cuts_graph_upload(cuts_hgraph h, int device, cuts_graph *out) {
     if (!h || !out) return set_error(CUTS_ERR_ARG, "null argument");
     *out = nullptr;

@@ -262,4 +262,53 @@ int write_graph_text(const std::string &path, const HostGraph &g) {
     return CUTS_OK;
 }
 
+// Binary CSR cache: "CUTSCSR1", n, arcs, symmetric flag, then out_off[n+1],
+// out_adj[arcs] and, for a directed graph, in_off[n+1], in_adj[arcs]
+// (little-endian u64 / u32).  Loading it skips text parsing and sorting.
+static const char kCsrMagic[8] = {'C', 'U', 'T', 'S', 'C', 'S', 'R', '1'};
+
+int save_graph_binary(const std::string &path, const HostGraph &g) {
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return set_error(CUTS_ERR_IO, "cannot write " + path);
+    const uint64_t hdr[3] = {g.n, g.arcs, g.symmetric ? 1ull : 0ull};
+    bool ok = std::fwrite(kCsrMagic, 1, 8, f) == 8 && std::fwrite(hdr, 8, 3, f) == 3;
+    auto put = [&](const void *p, size_t sz, size_t cnt) {
+        ok = ok && (cnt == 0 || std::fwrite(p, sz, cnt, f) == cnt);
+    };
+    put(g.out_off.data(), 8, size_t(g.n) + 1);
+    put(g.out_adj.data(), 4, g.arcs);
+    if (!g.symmetric) {
+        put(g.in_off.data(), 8, size_t(g.n) + 1);
+        put(g.in_adj.data(), 4, g.arcs);
+    }
+    std::fclose(f);
+    return ok ? CUTS_OK : set_error(CUTS_ERR_IO, "short write to " + path);
+}
+
+int load_graph_binary(const std::string &path, HostGraph &g) {
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return set_error(CUTS_ERR_IO, "load graph file failed: " + path);
+    std::unique_ptr<FILE, int (*)(FILE *)> hold(f, std::fclose);
+    char magic[8];
+    uint64_t hdr[3];
+    if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCsrMagic, 8) != 0 ||
+        std::fread(hdr, 8, 3, f) != 3 || hdr[0] > 0xFFFFFFFFull)
+        return set_error(CUTS_ERR_PARSE, "not a cuts binary CSR file: " + path);
+    g = HostGraph();
+    g.n = uint32_t(hdr[0]);
+    g.arcs = hdr[1];
+    g.symmetric = hdr[2] != 0;
+    auto get = [&](auto &vec, size_t cnt) {
+        vec.resize(cnt);
+        return cnt == 0 || std::fread(vec.data(), sizeof(vec[0]), cnt, f) == cnt;
+    };
+    bool ok = get(g.out_off, size_t(g.n) + 1) && get(g.out_adj, g.arcs);
+    if (ok && !g.symmetric) ok = get(g.in_off, size_t(g.n) + 1) && get(g.in_adj, g.arcs);
+    if (!ok || g.out_off[0] != 0 || g.out_off[g.n] != g.arcs)
+        return set_error(CUTS_ERR_PARSE, "truncated or inconsistent binary CSR: " + path);
+    for (uint64_t a = 0; a < g.arcs; ++a)
+        if (g.out_adj[a] >= g.n) return set_error(CUTS_ERR_PARSE, "arc endpoint out of range in " + path);
+    return CUTS_OK;
+}
+
 }  // namespace cuts

@@ -46,6 +46,9 @@ int graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj,
                    const uint64_t *in_off, const uint32_t *in_adj, HostGraph &g);
 // Writes the reference text format.
 int write_graph_text(const std::string &path, const HostGraph &g);
+// Binary CSR cache (skips parsing and sorting on reload).
+int save_graph_binary(const std::string &path, const HostGraph &g);
+int load_graph_binary(const std::string &path, HostGraph &g);
 
 // Query graph with its matching order and P/C join lists over level
 // positions (graph.cpp:94-133).

@@ -68,6 +68,11 @@ int cuts_hgraph_csr(cuts_hgraph h, uint64_t *out_off, uint32_t *out_adj, uint64_
                     uint32_t *in_adj);
 /* Write the reference text format (line 1 = V, then "s<TAB>t"). */
 int cuts_hgraph_write(cuts_hgraph h, const char *path);
+/* Binary CSR cache of a host graph: saving once makes later loads skip text
+ * parsing and sorting (the reference re-parses the text on every run,
+ * util.cpp:19-52). */
+int cuts_hgraph_save_binary(cuts_hgraph h, const char *path);
+int cuts_hgraph_load_binary(const char *path, cuts_hgraph *out);
 /* Make a host graph resident on `device` (the host graph stays valid).
  * Replaces malloc_graph_gpu_memory (gpu_memory_allocation.cu:26-37). */
 int cuts_graph_upload(cuts_hgraph h, int device, cuts_graph *out);

@@ -217,3 +217,44 @@ def test_plan_fuse_conditions():
     # 4-cycle: the last vertex does not join the previous one's lists -> no fuse
     c4 = cb.Query.from_arcs(*cb.named_query_arcs("4-cycle"))
     assert all(l["fuse"] == 0 for l in c4.plan_levels(True, 0)[0])
+
+
+def test_binary_csr_cache(tmp_path):
+    for h in (cb.HostGraph.erdos_renyi(5000, 0.002, seed=3),):
+        p = str(tmp_path / "g.csr")
+        h.save_binary(p)
+        h2 = cb.HostGraph.load_binary(p)
+        assert h2.info() == h.info()
+        for a, b in zip(h.csr(), h2.csr()):
+            assert (a is None and b is None) or np.array_equal(a, b)
+    # directed graph round trip through text then binary
+    p_txt = str(tmp_path / "d.txt")
+    with open(p_txt, "w") as f:
+        f.write("5\n0\t1\n1\t2\n2\t0\n3\t4\n")
+    d = cb.HostGraph.load(p_txt)
+    d.save_binary(str(tmp_path / "d.csr"))
+    d2 = cb.HostGraph.load_binary(str(tmp_path / "d.csr"))
+    assert d2.info() == d.info() and not d2.info()[2]
+    for a, b in zip(d.csr(), d2.csr()):
+        assert np.array_equal(a, b)
+    with open(tmp_path / "bad.csr", "wb") as f:
+        f.write(b"NOTACSR!")
+    with pytest.raises(cb.CutsError) as e:
+        cb.HostGraph.load_binary(str(tmp_path / "bad.csr"))
+    assert e.value.code == cb.ERR_PARSE
+
+
+def test_converters(tmp_path):
+    from cuts_b200 import convert
+    snap = tmp_path / "s.txt"
+    snap.write_text("# comment line\n# another\n0\t5\n5\t0\n2\t3\n")
+    n = convert.snap_to_cuts(str(snap), str(tmp_path / "s.g"))
+    assert n == 6
+    h = cb.HostGraph.load(str(tmp_path / "s.g"))
+    assert h.info()[:2] == (6, 3)
+    q = tmp_path / "q.g"
+    q.write_text("3\n0\t1\n1\t2\n2\t0\n")
+    convert.cuts_to_gsi(str(q), str(tmp_path / "q.gsi"))
+    lines = (tmp_path / "q.gsi").read_text().splitlines()
+    assert lines[0] == "t # 0" and lines[1] == "3 3 1 1" and lines[-1] == "t # -1"
+    assert lines[2:5] == ["v 0 1", "v 1 1", "v 2 1"] and lines[5] == "e 0 1 1"
