@@ -103,10 +103,19 @@ static uint32_t joins_at(const Query &q, const uint32_t *order, uint32_t i) {
     return nj;
 }
 
+// Work of level i+1 per entry of L_i: one probe sequence per joined list,
+// except a last level with a single joined list and no self-loop, which the
+// engine counts by list arithmetic (and folds into the level before).
+static double level_cost(const Query &q, const uint32_t *order, uint32_t i) {
+    const uint32_t nj = joins_at(q, order, i + 1);
+    if (i + 2 == q.k && nj == 1 && !q.self_loop(order[i + 1])) return kClosedFormCost;
+    return 1.0 + nj;
+}
+
 double predicted_work(const Query &q, const uint32_t *order, const float *pred) {
     double w = 0;
     for (uint32_t i = 0; i + 1 < q.k; ++i)
-        w += std::expm1(double(std::max(pred[i], 0.f))) * (1.0 + joins_at(q, order, i + 1));
+        w += std::expm1(double(std::max(pred[i], 0.f))) * level_cost(q, order, i);
     return w;
 }
 

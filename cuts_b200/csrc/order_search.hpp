@@ -23,7 +23,11 @@ DegreeStats degree_stats(const HostGraph &g);
 void step_features(const Query &q, const DegreeStats &ds, const uint32_t *order, uint32_t i,
                    float parent_log, float *f);
 
-// sum_{i<k-1} (exp(pred_i) - 1) * (1 + joins at level i+1)
+// Relative cost per parent of a closed-form last level (counted, not scanned).
+constexpr double kClosedFormCost = 0.1;
+
+// sum_{i<k-1} (exp(pred_i) - 1) * cost of level i+1 per parent: 1 + its
+// joined lists, or kClosedFormCost for a closed-form last level
 double predicted_work(const Query &q, const uint32_t *order, const float *pred);
 
 struct OrderSearchOptions {

@@ -112,9 +112,18 @@ def prediction_error(m: "cb.Mlp", X: np.ndarray, y: np.ndarray) -> float:
     return float(np.mean(np.abs(m.predict(X) - y)))
 
 
+CLOSED_FORM_COST = 0.1  # per parent, a closed-form last level (as the order search)
+
+
 def work(levels: Sequence[int], k: int, joins: Sequence[int]) -> float:
-    """Measured work of an order: sum over stored levels of |L_i| x (1 + joins at i+1)."""
-    return float(sum(levels[i] * (1 + joins[i + 1]) for i in range(k - 1)))
+    """Measured work of an order: sum over levels of |L_i| x the next level's
+    per-parent cost (1 + its joined lists; CLOSED_FORM_COST for a last level
+    with one joined list, which the engine counts by list arithmetic)."""
+    def cost(i):
+        if i + 2 == k and joins[i + 1] == 1:
+            return CLOSED_FORM_COST
+        return 1 + joins[i + 1]
+    return float(sum(levels[i] * cost(i) for i in range(k - 1)))
 
 
 def joins_of(q: "cb.Query") -> List[int]:
