@@ -98,6 +98,7 @@ _SIGS = {
                                     C.POINTER(_vp)]),
     "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "cuts_batch_info": (C.c_int, [_vp, _u64p, _u32p]),
+    "cuts_batch_set_query_budget": (C.c_int, [_vp, C.c_double]),
     "cuts_batch_free": (None, [_vp]),
     "cuts_count_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.POINTER(_vp), C.c_uint32,
                                      C.c_uint32, _vp, _vp]),
@@ -407,7 +408,9 @@ class Graph:
         return CountResult(cnt.value, ms.value, [int(x) for x in lv])
 
     def count_budget(self, q: Query, budget_ms: float, chunks: int = 1, flags: int = 0):
-        """(CountResult, finished): stops between chunks once budget_ms has passed."""
+        """(CountResult, finished): stops once budget_ms has passed (the host
+        checks between chunks; the kernels take no more work after budget_ms
+        of device time)."""
         cnt, ms = C.c_uint64(), C.c_float()
         lv = np.zeros(q.k, np.uint64)
         rc = lib().cuts_count_budget(self._h, q._h, chunks, flags, budget_ms, C.byref(cnt),
@@ -550,6 +553,11 @@ class Batch:
         ms = C.c_float()
         _check(lib().cuts_batch_run(self._h, budget_ms, _ptr(counts, _u64p), status, C.byref(ms)))
         return [int(x) for x in counts[:self.nq]], list(status)[:self.nq], ms.value
+
+    def set_query_budget(self, ms: float) -> None:
+        """Each query may use `ms` of the whole GPU in later runs; a query past
+        it reports ERR_BUDGET while the others carry on (0 = no limit)."""
+        _check(lib().cuts_batch_set_query_budget(self._h, ms))
 
     def info(self):
         t, b = C.c_uint64(), C.c_uint32()

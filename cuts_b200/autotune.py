@@ -22,13 +22,15 @@ BLOCKS = (0, 4)
 
 def tune_batch(g: "cb.Graph", queries: Sequence["cb.Query"], flags: int = 0,
                grains: Iterable[int] = GRAINS, grabs: Iterable[int] = GRABS,
-               blocks: Iterable[int] = BLOCKS, reps: int = 3, budget_ms: float = 0.0):
+               blocks: Iterable[int] = BLOCKS, reps: int = 3, budget_ms: float = 0.0,
+               query_budget_ms: float = 0.0):
     """Returns (best (grain, grab, blocks), {config: median ms})."""
     times: Dict[Tuple[int, int, int], float] = {}
     ref: Optional[List[int]] = None
-    if budget_ms > 0:
-        # tune on the queries that finish within the budget in the default shape
+    if budget_ms > 0 or query_budget_ms > 0:
+        # tune on the queries that finish within the budgets in the default shape
         b = g.batch(queries, flags=flags)
+        b.set_query_budget(query_budget_ms)
         _, status, _ = b.run(budget_ms)
         b.close()
         queries = [q for q, s in zip(queries, status) if s == 0]

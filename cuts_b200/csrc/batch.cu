@@ -211,7 +211,8 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
         const unsigned long long *__restrict__ pref2, uint32_t grain, uint32_t tgrab,
         unsigned long long *__restrict__ task_ctr, uint32_t *__restrict__ stop,
         unsigned long long *__restrict__ counts, uint32_t *__restrict__ aborted,
-        unsigned long long budget_ns) {
+        unsigned long long budget_ns, unsigned long long *__restrict__ qtime,
+        unsigned long long qlimit) {
     __shared__ BWarp ws[kBW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Ctx c{g, nullptr, &ws[warp], lane};
@@ -243,6 +244,21 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
                 if (lane == 0) { atomicOr(stop, 1u); aborted[cur] = 1; }
                 continue;
             }
+            // per-query limit: a query past its share of warp time is dropped,
+            // and the work counter skips the rest of its tasks
+            if (qlimit) {
+                uint32_t skip = 0;
+                if (lane == 0) {
+                    skip = reinterpret_cast<volatile uint32_t *>(aborted)[cur] ||
+                           reinterpret_cast<volatile unsigned long long *>(qtime)[cur] > qlimit;
+                    if (skip) {
+                        aborted[cur] = 1;
+                        atomicMax(task_ctr, qbase[cur + 1]);
+                    }
+                }
+                if (__shfl_sync(kFullMask, skip, 0)) continue;
+            }
+            const unsigned long long task_start = qlimit ? global_ns() : 0;
             const BQuery &Q = *c.Q;
             const unsigned long long local = t - qbase[cur];
             const unsigned long long *pref = Q.type == 0 ? pref0 : (Q.type == 1 ? pref1 : pref2);
@@ -295,7 +311,7 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
             }
             // depth-first over levels 1..k-2, counting level k-1
             uint32_t d = 1;
-            bool abandoned = false;
+            bool abandoned = false, dropped = false;
             while (d >= 1) {
                 if (c.S->bi[d] < c.S->nb[d]) {
                     const uint32_t v = c.S->buf[d][c.S->bi[d]];
@@ -310,7 +326,13 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
                     else if (d + 3 == Q.k && Q.lv[d + 1].fold) qcount += count_level_fold(c, d + 1);
                     else ++d;
                 } else if (c.S->x[d] < c.S->xend[d]) {
-                    if (*vstop || global_ns() > deadline) { abandoned = true; break; }
+                    const unsigned long long now = global_ns();
+                    if (*vstop || now > deadline) { abandoned = true; break; }
+                    if (qlimit && reinterpret_cast<volatile unsigned long long *>(qtime)[cur] +
+                                          (now - task_start) > qlimit) {
+                        dropped = true;
+                        break;
+                    }
                     refill(c, d);
                 } else {
                     --d;
@@ -319,6 +341,10 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
             if (abandoned && lane == 0) {
                 atomicOr(stop, 1u);
                 aborted[cur] = 1;
+            }
+            if (qlimit && lane == 0) {
+                atomicAdd(&qtime[cur], global_ns() - task_start);
+                if (dropped) aborted[cur] = 1;
             }
         }
     }
@@ -367,6 +393,7 @@ void Batch::destroy() {
     cudaFree(d_qbase);
     cudaFree(d_counts);
     cudaFree(d_aborted);
+    cudaFree(d_qtime);
     cudaFree(d_ctr);
     cudaFreeHost(h_counts);
     cudaFreeHost(h_aborted);
@@ -377,6 +404,7 @@ void Batch::destroy() {
     d_qbase = nullptr;
     d_counts = nullptr;
     d_aborted = nullptr;
+    d_qtime = nullptr;
     d_ctr = nullptr;
     h_counts = nullptr;
     h_aborted = nullptr;
@@ -453,6 +481,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
     BCK(cudaMalloc(&d_qbase, sizeof(unsigned long long) * qbase.size()));
     BCK(cudaMalloc(&d_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1)));
     BCK(cudaMalloc(&d_aborted, sizeof(uint32_t) * std::max<uint32_t>(nb, 1)));
+    BCK(cudaMalloc(&d_qtime, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1)));
     BCK(cudaMalloc(&d_ctr, sizeof(unsigned long long) * 2));
     BCK(cudaMallocHost(&h_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1)));
     BCK(cudaMallocHost(&h_aborted, sizeof(uint32_t) * std::max<uint32_t>(nb, 1)));
@@ -466,7 +495,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
 }
 
 int Batch::capture(unsigned long long budget_ns) {
-    if (exec && budget_ns == captured_budget) return CUTS_OK;
+    if (exec && budget_ns == captured_budget && query_budget_ms == captured_query_budget) return CUTS_OK;
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
     if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
     int bps = 0;
@@ -483,13 +512,16 @@ int Batch::capture(unsigned long long budget_ns) {
     BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1), s);
     cudaMemsetAsync(d_aborted, 0, sizeof(uint32_t) * std::max<uint32_t>(nb, 1), s);
+    cudaMemsetAsync(d_qtime, 0, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1), s);
+    const unsigned long long qlimit =
+        query_budget_ms > 0 ? (unsigned long long)(query_budget_ms * 1e6 * double(blocks) * kBW) : 0ull;
     cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 2, s);
     if (nb) {
         k_batch<<<blocks, kBW * 32, 0, s>>>(
             DevView{g->out_info, g->in_info, g->adj, g->n}, d_queries, nb, d_qbase, g->batch_vsorted,
             pref, g->symmetric ? pref : pref + stride, g->symmetric ? pref : pref + 2 * stride, tune.grain,
             tune.tasks_per_grab, d_ctr, reinterpret_cast<uint32_t *>(d_ctr + 1), d_counts, d_aborted,
-            budget_ns);
+            budget_ns, d_qtime, qlimit);
     }
     cudaMemcpyAsync(h_counts, d_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1),
                     cudaMemcpyDeviceToHost, s);
@@ -501,6 +533,7 @@ int Batch::capture(unsigned long long budget_ns) {
     graph = gr;
     BCK(cudaGraphInstantiate(&exec, graph, 0));
     captured_budget = budget_ns;
+    captured_query_budget = query_budget_ms;
     launch_blocks = blocks;
     return CUTS_OK;
 }
@@ -532,6 +565,7 @@ int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int>
         CountResult r;
         CountOptions opt;
         opt.flags = flags;
+        opt.budget_ms = query_budget_ms;
         rc = device_count(*g, *queries[i], opt, r);
         if (rc) {
             status[i] = rc;

@@ -52,11 +52,14 @@ struct Batch {
     BQuery *d_queries = nullptr;
     unsigned long long *d_qbase = nullptr, *d_counts = nullptr, *d_ctr = nullptr;
     uint32_t *d_aborted = nullptr;
+    unsigned long long *d_qtime = nullptr;  // warp-ns spent per query (per-query limit)
+    double query_budget_ms = 0;             // per-query limit in whole-GPU ms (0 = none)
     unsigned long long *h_counts = nullptr, *h_ctr = nullptr;
     uint32_t *h_aborted = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long captured_budget = ~0ull;
+    double captured_query_budget = -1;
     uint32_t launch_blocks = 0;
 
     int create(DeviceGraph &g, const std::vector<const Query *> &qs, uint32_t flags,
@@ -64,6 +67,10 @@ struct Batch {
     // budget_ms > 0 stops the launch after that much device time; queries not
     // finished report CUTS_ERR_BUDGET.
     int run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int> &status, float *ms);
+    // Each query may use query_budget_ms of the whole GPU (its warp time,
+    // summed over the launch's warps, up to query_budget_ms x warps); a query
+    // past it reports CUTS_ERR_BUDGET and the others carry on.  0 = no limit.
+    void set_query_budget(double ms) { query_budget_ms = ms; }
     void destroy();
 
   private:

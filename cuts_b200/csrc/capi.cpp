@@ -564,6 +564,12 @@ int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status
     })());
 }
 
+int cuts_batch_set_query_budget(cuts_batch b, double ms) {
+    if (!b || !(ms >= 0)) return set_error(CUTS_ERR_ARG, "bad batch or budget");
+    b->b.set_query_budget(ms);
+    return CUTS_OK;
+}
+
 int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks) {
     if (!b) return set_error(CUTS_ERR_ARG, "null batch");
     if (tasks) *tasks = b->b.total_tasks;

@@ -58,10 +58,31 @@ struct RunParams {
     uint32_t stored;   // levels kept in HBM: k-1 when counting, k when dumping
     uint32_t fuse_stride;  // words per warp row of the fused kernel's scratch
     uint32_t *fuse_scratch;
+    uint32_t *fuse_big;    // the fused kernel's deferred parents (counters, arrays, pool)
+    uint32_t fuse_big_cap;
+    uint32_t fuse_pool_words;
     uint32_t *vert[kMaxK];
     uint32_t *par[kMaxK];
     uint32_t *ub[kMaxK];
+    // device-time budget: kernels take no more work once budget_ns has
+    // passed since *stamp (written by k_roots) and raise *over instead
+    unsigned long long budget_ns;
+    unsigned long long *stamp;
+    uint32_t *over;
 };
+
+// Absolute device-clock deadline of a budgeted run (0 = none).
+__device__ __forceinline__ unsigned long long run_deadline(const RunParams *rp) {
+    const unsigned long long b = rp->budget_ns;
+    return b ? *rp->stamp + b : 0ull;
+}
+
+// True (and the run flagged) once the deadline has passed; lane 0 calls it.
+__device__ __forceinline__ bool past_deadline(const RunParams *rp, unsigned long long deadline) {
+    if (!deadline || global_ns() <= deadline) return false;
+    atomicOr(rp->over, 1u);
+    return true;
+}
 
 enum Mode { kExpand = 0, kCountMode = 1, kBytesMode = 2 };
 
@@ -78,6 +99,7 @@ __global__ void k_roots(DevView g, const RunParams *__restrict__ rp, uint32_t sh
         for (uint32_t t = 0; t < P.lv[1].nj; ++t) (P.lv[1].jdir[t] ? use_in : use_out) = true;
     uint32_t *vert0 = rp->vert[0], *ub0 = rp->ub[0];
     const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rp->budget_ns) *rp->stamp = global_ns();
     for (uint32_t base = blockIdx.x * blockDim.x; base < g.n; base += gridDim.x * blockDim.x) {
         const uint32_t u = base + threadIdx.x;
         bool ok = false;
@@ -160,6 +182,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
     uint32_t obn = 0;           // staged outputs (warp-uniform)
     unsigned long long local = 0;
     const uint32_t total = pb - pa;
+    const unsigned long long deadline = run_deadline(rp);
 
     auto flush = [&]() {
         if constexpr (MODE != kExpand) return;
@@ -182,7 +205,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
 
     while (true) {
         uint32_t start = 0;
-        if (lane == 0) start = atomicAdd(cursor, grain);
+        if (lane == 0) start = past_deadline(rp, deadline) ? total : atomicAdd(cursor, grain);
         start = __shfl_sync(kFull, start, 0);
         if (start >= total) break;
         const uint32_t end = min(start + grain, total);
@@ -386,6 +409,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     const bool fold = MODE != kExpand && sL.fold;
     const bool fold_guar_c = fold && ((sN.guar_mask >> lvl) & 1u);
     const uint32_t total = pb - pa;
+    const unsigned long long deadline = run_deadline(rp);
     unsigned long long local = 0, local2 = 0;
     uint32_t obn = 0;
 
@@ -410,7 +434,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
 
     while (true) {
         uint32_t start = 0;
-        if (lane == 0) start = atomicAdd(cursor, 32u);
+        if (lane == 0) start = past_deadline(rp, deadline) ? total : atomicAdd(cursor, 32u);
         start = __shfl_sync(kFullMask, start, 0);
         if (start >= total) break;
         const uint32_t p = pa + start + lane;
@@ -614,23 +638,40 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
 // a vertex s chosen at p are the members t of p's candidate set S (same
 // parent) that lie in s's list.  One warp per parent at level p - 1: build S
 // once (the usual scan of the shortest joined list, membership in the
-// others, ballot compaction) into the warp's scratch row, then for every s
-// in S intersect S with s's list -- iterating whichever of the two is
-// shorter, lane-parallel, with lower-bound probes into the other -- and
-// count (or, for a folded c, add the last level's closed form per t).  Level
-// p is never written to the trie.
-constexpr int kZW = 4;  // warps per block
+// others, ballot compaction) into the warp's scratch row, then intersect S
+// with the list of every s in S, 32 vertices s at a time (one per lane), and
+// count (or, for a folded c, add the last level's closed form per t).
+// Level p is never written to the trie.
+//
+// The work of one parent grows like |S|^2, so a hub parent would keep one
+// warp busy long after the others finish.  Phase 1 therefore defers every
+// parent with |S| > kBigS: it copies S into a pool and records the parent;
+// phase 2 (a second launch, after a one-block scan of the deferred parents'
+// group counts) hands out their groups of 32 vertices s to all warps.
+constexpr int kZW = 4;          // warps per block
+constexpr uint32_t kBigS = 256;  // default |S| above which a parent is split
+
+// Parents deferred by phase 1 and their saved candidate sets.
+struct FusedBig {
+    unsigned long long *n;  // [0] entries appended, [1] pool words taken
+    uint32_t *gi;           // parent index (in L_{p-1}) of each entry
+    uint32_t *soff;         // offset of its S in the pool
+    uint32_t *ns;           // |S|
+    uint32_t *pref;         // inclusive prefix sum of groups of 32 (phase 2)
+    uint32_t *pool;
+    uint32_t cap;
+    unsigned long long pool_words;
+};
 
 template <int MODE>
 __global__ void __launch_bounds__(kZW * 32)
-k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb,
-        uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride,
+k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb, uint32_t phase,
+        uint32_t split, uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride, FusedBig big,
         unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,
         unsigned long long *__restrict__ acc_p) {
     __shared__ LevelPlan sP, sC, sF;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
-    __shared__ uint32_t s_k;
     __shared__ uint32_t wm[kZW][kMaxK];
     __shared__ uint32_t joff[kZW][kMaxJ], jdeg[kZW][kMaxJ];
     __shared__ uint32_t xoff[kZW][kMaxJ], xdeg[kZW][kMaxJ];
@@ -650,13 +691,12 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             s_vert[threadIdx.x] = rp->vert[threadIdx.x];
             s_par[threadIdx.x] = rp->par[threadIdx.x];
         }
-        if (threadIdx.x == 0) s_k = rp->plan.k;
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lanemask_lt = (1u << lane) - 1;
     uint32_t *my_m = wm[warp];
-    uint32_t *S = scratch + size_t(blockIdx.x * kZW + warp) * stride;
+    uint32_t *const row = scratch + size_t(blockIdx.x * kZW + warp) * stride;
     const uint32_t c = p + 1;
     // the counted level c is folded when level c carries the fold flag
     const bool cfold = sC.fold != 0;
@@ -666,100 +706,162 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
     const uint32_t below = (1u << p) - 1;
     const bool c_gt_s = (sC.gt_mask >> p) & 1u, c_lt_s = (sC.lt_mask >> p) & 1u;
     const bool fguar_t = cfold && ((sF.guar_mask >> c) & 1u);
+    // an extra list of c on position p itself changes with s: per-s loop
+    bool extra_on_p = false;
+    for (uint32_t t = 0; t < sC.nj; ++t)
+        if (((extra >> t) & 1u) && sC.jpos[t] == p) extra_on_p = true;
     unsigned long long local = 0, local_c = 0, local_p = 0;
     uint32_t cached_q = kFullMask;
-    const uint32_t total = pb - pa;
+    const bool phase2 = phase == 2;
+    uint32_t nbig = 0, total = pb - pa;
+    if (phase2) {
+        const unsigned long long n0 = big.n[0];
+        nbig = n0 < big.cap ? uint32_t(n0) : big.cap;
+        total = nbig ? big.pref[nbig - 1] : 0;
+    }
+    const unsigned long long deadline = run_deadline(rp);
     auto probes = [](uint32_t len) { return 32u - __clz(len | 1u); };
 
-    while (true) {
-        uint32_t gi = 0;
-        if (lane == 0) gi = atomicAdd(cursor, 1u);
-        gi = __shfl_sync(kFullMask, gi, 0);
-        if (gi >= total) break;
-        const uint32_t q0 = pa + gi;
-        if (lane == 0) {  // matched vertices of the parent at level p-1
-            my_m[p - 1] = s_vert[p - 1][q0];
-            if (p >= 2) {
-                uint32_t q = s_par[p - 1][q0];
-                if (q != cached_q) {
-                    cached_q = q;
-                    for (int j = int(p) - 2; j >= 0; --j) {
-                        my_m[j] = s_vert[j][q];
-                        if (j > 0) q = s_par[j][q];
+    // level c for the vertices s = S[i0 .. i0+32) of one parent
+    auto group = [&](const uint32_t *S, uint32_t ns, uint32_t i0, uint32_t lo_c, uint32_t hi_c) {
+        if (!extra_on_p) {
+            // one s per lane; the 32 (s, t) sequences are concatenated and
+            // spread over all lanes, as in k_level_flat
+            const uint32_t i = i0 + lane;
+            // the iterated range starts at itb (in S when iters, else in the
+            // adjacency array); the probed one is [ostart, oend) of S or of
+            // the list at ooff
+            uint32_t sv = kFullMask, itb = 0, ooff = 0, ostart = 0, oend = 0, nit = 0, iters = 1;
+            uint32_t fbase = 0, foff = 0, fdeg = 0, flo = 0, fhi = kFullMask;
+            if (i < ns) {
+                sv = S[i];
+                const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
+                const uint32_t lsoff = is.x, ds = is.y;
+                uint32_t lo_t = lo_c, hi_t = hi_c;
+                if (c_gt_s) lo_t = max(lo_t, sv + 1);
+                if (c_lt_s) hi_t = min(hi_t, sv);
+                const uint32_t ts = lo_t ? lbound(S, ns, lo_t) : 0;
+                const uint32_t te = hi_t != kFullMask ? lbound(S, ns, hi_t) : ns;
+                const uint32_t *Ls = g.adj + lsoff;
+                const uint32_t ls0 = lo_t ? lbound(Ls, ds, lo_t) : 0;
+                const uint32_t ls1 = hi_t != kFullMask ? lbound(Ls, ds, hi_t) : ds;
+                const uint32_t nS = te > ts ? te - ts : 0, nL = ls1 > ls0 ? ls1 - ls0 : 0;
+                iters = nS <= nL ? 1u : 0u;  // iterate the shorter side
+                nit = iters ? nS : nL;
+                itb = iters ? ts : lsoff + ls0;
+                ooff = iters ? lsoff : 0;
+                ostart = iters ? ls0 : ts;
+                oend = iters ? ls1 : te;
+                if (cfold) {
+                    // folded last level: f_base(s) = |window of L_F| - matched in it
+                    const uint32_t jf = sF.jpos[0];
+                    const uint32_t u = jf == p ? sv : my_m[jf];
+                    const uint2 inf = sF.jdir[0] ? g.in_info[u] : g.out_info[u];
+                    foff = inf.x;
+                    fdeg = inf.y;
+                    for (uint32_t msk = sF.gt_mask; msk; msk &= msk - 1) {
+                        const uint32_t j = __ffs(msk) - 1;
+                        flo = max(flo, (j == p ? sv : my_m[j]) + 1);
+                    }
+                    for (uint32_t msk = sF.lt_mask; msk; msk &= msk - 1) {
+                        const uint32_t j = __ffs(msk) - 1;
+                        fhi = min(fhi, j == p ? sv : my_m[j]);
+                    }
+                    const uint32_t *fl = g.adj + foff;
+                    const uint32_t ws = flo ? lbound(fl, fdeg, flo) : 0;
+                    const uint32_t we = fhi != kFullMask ? lbound(fl, fdeg, fhi) : fdeg;
+                    uint32_t sub = 0;
+                    for (uint32_t j = 0; j <= p; ++j) {
+                        const uint32_t mj = j == p ? sv : my_m[j];
+                        if (mj >= flo && mj < fhi && (((sF.guar_mask >> j) & 1u) || contains(fl, fdeg, mj))) ++sub;
+                    }
+                    fbase = (we > ws ? we - ws : 0) - sub;
+                }
+                if (MODE == kBytesMode)
+                    local += 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iters ? ds : nS) +
+                             (sig_c ? 8ull * nit : 0) + (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
+            }
+            if (MODE == kBytesMode) return;
+            uint32_t incl = nit;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t ftotal = __shfl_sync(kFullMask, incl, 31);
+            const uint32_t excl = incl - nit;
+            uint32_t gal_owner = kFullMask, gal = 0;
+            for (uint32_t fstep = 0; fstep < ftotal; fstep += 32) {
+                const uint32_t f = fstep + lane;
+                uint32_t owner = 0;
+                #pragma unroll
+                for (int step = 16; step; step >>= 1) {
+                    const uint32_t probe = __shfl_sync(kFullMask, incl, int(owner + step - 1));
+                    if (probe <= f) owner += step;
+                }
+                owner = min(owner, 31u);
+                const int ow = int(owner);
+                const uint32_t o_excl = __shfl_sync(kFullMask, excl, ow);
+                const uint32_t o_sv = __shfl_sync(kFullMask, sv, ow);
+                const uint32_t o_itb = __shfl_sync(kFullMask, itb, ow);
+                const uint32_t o_ooff = __shfl_sync(kFullMask, ooff, ow);
+                const uint32_t o_ostart = __shfl_sync(kFullMask, ostart, ow);
+                const uint32_t o_oend = __shfl_sync(kFullMask, oend, ow);
+                const uint32_t o_iters = __shfl_sync(kFullMask, iters, ow);
+                uint32_t o_fbase = 0, o_foff = 0, o_fdeg = 0, o_flo = 0, o_fhi = 0;
+                if (cfold) {
+                    o_fbase = __shfl_sync(kFullMask, fbase, ow);
+                    o_foff = __shfl_sync(kFullMask, foff, ow);
+                    o_fdeg = __shfl_sync(kFullMask, fdeg, ow);
+                    o_flo = __shfl_sync(kFullMask, flo, ow);
+                    o_fhi = __shfl_sync(kFullMask, fhi, ow);
+                }
+                bool ok = f < ftotal;
+                if (owner != gal_owner) {
+                    gal_owner = owner;
+                    gal = o_ostart;
+                }
+                uint32_t t = 0;
+                if (ok) {
+                    const uint32_t y = f - o_excl;
+                    if (o_iters) {
+                        t = S[o_itb + y];
+                        const uint32_t *Lo = g.adj + o_ooff;
+                        const uint32_t pos = lbound_from(Lo, o_oend, gal, t);
+                        gal = pos;
+                        ok = pos < o_oend && __ldg(Lo + pos) == t;
+                    } else {
+                        t = __ldg(g.adj + o_itb + y);
+                        const uint32_t pos = lbound_from(S, o_oend, gal, t);
+                        gal = pos;
+                        ok = pos < o_oend && S[pos] == t;
+                    }
+                }
+                if (ok && t == o_sv) ok = false;
+                if (ok && extra)
+                    for (uint32_t tt = 0; tt < sC.nj; ++tt)
+                        if ((extra >> tt) & 1u)
+                            if (!contains(g.adj + xoff[warp][tt], xdeg[warp][tt], t)) { ok = false; break; }
+                if (ok && sig_c) {
+                    const uint2 o = g.out_info[t], i2 = g.in_info[t];
+                    ok = i2.y >= sC.qin && o.y >= sC.qout;
+                }
+                if (ok) {
+                    ++local_c;
+                    if (cfold) {
+                        const bool h = t >= o_flo && t < o_fhi && (fguar_t || contains(g.adj + o_foff, o_fdeg, t));
+                        local += o_fbase - (h ? 1u : 0u);
+                    } else {
+                        ++local;
                     }
                 }
             }
+            __syncwarp();
+            return;
         }
-        __syncwarp();
-        // level p: joined lists, the shortest supplies S
-        const uint32_t njp = sP.nj;
-        uint32_t md = kFullMask, mo = 0;
-        if (uint32_t(lane) < njp) {
-            const uint32_t u = my_m[sP.jpos[lane]];
-            const uint2 inf = sP.jdir[lane] ? g.in_info[u] : g.out_info[u];
-            mo = inf.x;
-            md = inf.y;
-            joff[warp][lane] = mo;
-            jdeg[warp][lane] = md;
-        }
-        uint32_t bd = md, bl = uint32_t(lane);
-        #pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const uint32_t od = __shfl_xor_sync(kFullMask, bd, o), ol = __shfl_xor_sync(kFullMask, bl, o);
-            if (od < bd || (od == bd && ol < bl)) { bd = od; bl = ol; }
-        }
-        const uint32_t moff = __shfl_sync(kFullMask, mo, int(bl)), mdeg = njp ? bd : 0, tmin = bl;
-        // extra lists of level c on positions below p: fixed for this parent
-        if (uint32_t(lane) < sC.nj && ((extra >> lane) & 1u) && sC.jpos[lane] < p) {
-            const uint32_t u = my_m[sC.jpos[lane]];
-            const uint2 inf = sC.jdir[lane] ? g.in_info[u] : g.out_info[u];
-            xoff[warp][lane] = inf.x;
-            xdeg[warp][lane] = inf.y;
-        }
-        __syncwarp();
-        uint32_t lo = 0, hi = kFullMask;
-        for (uint32_t msk = sP.gt_mask; msk; msk &= msk - 1) lo = max(lo, my_m[__ffs(msk) - 1] + 1);
-        for (uint32_t msk = sP.lt_mask; msk; msk &= msk - 1) hi = min(hi, my_m[__ffs(msk) - 1]);
-        const uint32_t *mlist = g.adj + moff;
-        const uint32_t s0 = lo ? lbound(mlist, mdeg, lo) : 0;
-        const uint32_t e0 = hi != kFullMask ? lbound(mlist, mdeg, hi) : mdeg;
-        uint32_t ns = 0;
-        for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
-            const uint32_t x = x0 + lane;
-            bool ok = x < e0;
-            const uint32_t v = ok ? __ldg(mlist + x) : 0;
-            if (ok)
-                for (uint32_t j = 0; j < p; ++j)
-                    if (v == my_m[j]) { ok = false; break; }
-            if (ok) {
-                const uint2 o = g.out_info[v], i = g.in_info[v];
-                ok = i.y >= sP.qin && o.y >= sP.qout;
-            }
-            if (ok)
-                for (uint32_t t = 0; t < njp; ++t) {
-                    if (t == tmin) continue;
-                    if (!contains(g.adj + joff[warp][t], jdeg[warp][t], v)) { ok = false; break; }
-                }
-            const unsigned m = __ballot_sync(kFullMask, ok);
-            if (ok) S[ns + __popc(m & lanemask_lt)] = v;
-            ns += __popc(m);
-            if (MODE == kBytesMode && lane == 0) {
-                uint32_t per = 8;
-                for (uint32_t t = 0; t < njp; ++t)
-                    if (t != tmin) per += 4 * probes(jdeg[warp][t]);
-                local += 4ull * min(32u, e0 - x0) + uint64_t(min(32u, e0 - x0)) * per;
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-            local_p += ns;
-            if (MODE == kBytesMode) local += 8ull * p + 8ull * njp + 4ull * ns;
-        }
-        // level c over the vertices s of S
-        uint32_t lo_c = 0, hi_c = kFullMask;
-        for (uint32_t msk = sC.gt_mask & below; msk; msk &= msk - 1) lo_c = max(lo_c, my_m[__ffs(msk) - 1] + 1);
-        for (uint32_t msk = sC.lt_mask & below; msk; msk &= msk - 1) hi_c = min(hi_c, my_m[__ffs(msk) - 1]);
-        for (uint32_t i = 0; i < ns; ++i) {
+        // a list of c on p itself: one s at a time, lane-parallel over t
+        const uint32_t iend = min(i0 + 32, ns);
+        for (uint32_t i = i0; i < iend; ++i) {
             const uint32_t sv = S[i];
             const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
             const uint32_t *Ls = g.adj + is.x;
@@ -770,13 +872,12 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             const uint32_t ts = lo_t ? lbound(S, ns, lo_t) : 0;
             const uint32_t te = hi_t != kFullMask ? lbound(S, ns, hi_t) : ns;
             if (ts >= te) continue;
-            // per-s extra lists of level c (joins on p in the other direction)
+            __syncwarp();
             if (uint32_t(lane) < sC.nj && ((extra >> lane) & 1u) && sC.jpos[lane] == p) {
                 const uint2 inf = sC.jdir[lane] ? g.in_info[sv] : g.out_info[sv];
                 xoff[warp][lane] = inf.x;
                 xdeg[warp][lane] = inf.y;
             }
-            // folded last level: f_base(s) = |window of L_F| - matched in it
             uint32_t fbase = 0, fdeg = 0, flo = 0, fhi = kFullMask;
             const uint32_t *fl = nullptr;
             if (cfold) {
@@ -851,7 +952,147 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                     }
                 }
             }
+        }
+        __syncwarp();
+    };
+
+    while (true) {
+        uint32_t gi = 0;
+        if (lane == 0) gi = past_deadline(rp, deadline) ? total : atomicAdd(cursor, 1u);
+        gi = __shfl_sync(kFullMask, gi, 0);
+        if (gi >= total) break;
+        // phase 2: work item gi is group grp of deferred parent b
+        uint32_t q0, b = 0, grp = 0;
+        if (!phase2) {
+            q0 = pa + gi;
+        } else {
+            uint32_t lo = 0, hi = nbig - 1;  // first b with pref[b] > gi
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (big.pref[mid] > gi) hi = mid; else lo = mid + 1;
+            }
+            b = lo;
+            grp = gi - (b ? big.pref[b - 1] : 0);
+            q0 = big.gi[b];
+        }
+        if (lane == 0) {  // matched vertices of the parent at level p-1
+            my_m[p - 1] = s_vert[p - 1][q0];
+            if (p >= 2) {
+                uint32_t q = s_par[p - 1][q0];
+                if (q != cached_q) {
+                    cached_q = q;
+                    for (int j = int(p) - 2; j >= 0; --j) {
+                        my_m[j] = s_vert[j][q];
+                        if (j > 0) q = s_par[j][q];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const uint32_t *S = row;
+        uint32_t ns = 0;
+        if (!phase2) {
+            // level p: joined lists, the shortest supplies S
+            const uint32_t njp = sP.nj;
+            uint32_t md = kFullMask, mo = 0;
+            if (uint32_t(lane) < njp) {
+                const uint32_t u = my_m[sP.jpos[lane]];
+                const uint2 inf = sP.jdir[lane] ? g.in_info[u] : g.out_info[u];
+                mo = inf.x;
+                md = inf.y;
+                joff[warp][lane] = mo;
+                jdeg[warp][lane] = md;
+            }
+            uint32_t bd = md, bl = uint32_t(lane);
+            #pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const uint32_t od = __shfl_xor_sync(kFullMask, bd, o), ol = __shfl_xor_sync(kFullMask, bl, o);
+                if (od < bd || (od == bd && ol < bl)) { bd = od; bl = ol; }
+            }
+            const uint32_t moff = __shfl_sync(kFullMask, mo, int(bl)), mdeg = njp ? bd : 0, tmin = bl;
             __syncwarp();
+            uint32_t lo = 0, hi = kFullMask;
+            for (uint32_t msk = sP.gt_mask; msk; msk &= msk - 1) lo = max(lo, my_m[__ffs(msk) - 1] + 1);
+            for (uint32_t msk = sP.lt_mask; msk; msk &= msk - 1) hi = min(hi, my_m[__ffs(msk) - 1]);
+            const uint32_t *mlist = g.adj + moff;
+            const uint32_t s0 = lo ? lbound(mlist, mdeg, lo) : 0;
+            const uint32_t e0 = hi != kFullMask ? lbound(mlist, mdeg, hi) : mdeg;
+            for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
+                const uint32_t x = x0 + lane;
+                bool ok = x < e0;
+                const uint32_t v = ok ? __ldg(mlist + x) : 0;
+                if (ok)
+                    for (uint32_t j = 0; j < p; ++j)
+                        if (v == my_m[j]) { ok = false; break; }
+                if (ok) {
+                    const uint2 o = g.out_info[v], i = g.in_info[v];
+                    ok = i.y >= sP.qin && o.y >= sP.qout;
+                }
+                if (ok)
+                    for (uint32_t t = 0; t < njp; ++t) {
+                        if (t == tmin) continue;
+                        if (!contains(g.adj + joff[warp][t], jdeg[warp][t], v)) { ok = false; break; }
+                    }
+                const unsigned m = __ballot_sync(kFullMask, ok);
+                if (ok) row[ns + __popc(m & lanemask_lt)] = v;
+                ns += __popc(m);
+                if (MODE == kBytesMode && lane == 0) {
+                    uint32_t per = 8;
+                    for (uint32_t t = 0; t < njp; ++t)
+                        if (t != tmin) per += 4 * probes(jdeg[warp][t]);
+                    local += 4ull * min(32u, e0 - x0) + uint64_t(min(32u, e0 - x0)) * per;
+                }
+            }
+            __syncwarp();
+            if (MODE == kCountMode && ns > split) {
+                // defer: save S in the pool for phase 2 (or keep it here when full)
+                unsigned long long off = 0;
+                uint32_t e = kFullMask;
+                if (lane == 0 && big.n[1] < big.pool_words) {
+                    off = atomicAdd(&big.n[1], (unsigned long long)ns);
+                    if (off + ns <= big.pool_words) {
+                        const unsigned long long e64 = atomicAdd(&big.n[0], 1ull);
+                        if (e64 < big.cap) e = uint32_t(e64);
+                    }
+                }
+                e = __shfl_sync(kFullMask, e, 0);
+                off = __shfl_sync(kFullMask, off, 0);
+                if (e != kFullMask) {
+                    for (uint32_t i = lane; i < ns; i += 32) big.pool[off + i] = row[i];
+                    if (lane == 0) {
+                        big.gi[e] = q0;
+                        big.soff[e] = uint32_t(off);
+                        big.ns[e] = ns;
+                    }
+                    __syncwarp();
+                    continue;
+                }
+            }
+            if (lane == 0) {
+                local_p += ns;
+                if (MODE == kBytesMode) local += 8ull * p + 8ull * njp + 4ull * ns;
+            }
+        } else {
+            S = big.pool + big.soff[b];
+            ns = big.ns[b];
+            if (lane == 0 && grp == 0) local_p += ns;
+        }
+        // extra lists of level c on positions below p: fixed for this parent
+        if (uint32_t(lane) < sC.nj && ((extra >> lane) & 1u) && sC.jpos[lane] < p) {
+            const uint32_t u = my_m[sC.jpos[lane]];
+            const uint2 inf = sC.jdir[lane] ? g.in_info[u] : g.out_info[u];
+            xoff[warp][lane] = inf.x;
+            xdeg[warp][lane] = inf.y;
+        }
+        __syncwarp();
+        // level c over the vertices s of S
+        uint32_t lo_c = 0, hi_c = kFullMask;
+        for (uint32_t msk = sC.gt_mask & below; msk; msk &= msk - 1) lo_c = max(lo_c, my_m[__ffs(msk) - 1] + 1);
+        for (uint32_t msk = sC.lt_mask & below; msk; msk &= msk - 1) hi_c = min(hi_c, my_m[__ffs(msk) - 1]);
+        if (!phase2) {
+            for (uint32_t i0 = 0; i0 < ns; i0 += 32) group(S, ns, i0, lo_c, hi_c);
+        } else {
+            group(S, ns, grp * 32, lo_c, hi_c);
         }
     }
     #pragma unroll
@@ -865,6 +1106,43 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             if (local_c) atomicAdd(acc_c, local_c);
             if (local_p) atomicAdd(acc_p, local_p);
         }
+    }
+}
+
+// Inclusive prefix sum of the deferred parents' group counts (one block).
+__global__ void __launch_bounds__(1024) k_fused_scan(FusedBig big) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const unsigned long long n0 = big.n[0];
+    const uint32_t n = n0 < big.cap ? uint32_t(n0) : big.cap;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t v = i < n ? (big.ns[i] + 31) / 32 : 0, x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFullMask, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t s = lane < int(blockDim.x / 32) ? wsum[lane] : 0;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFullMask, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        const uint32_t pre = carry + (w ? wsum[w - 1] : 0) + x;
+        if (i < n) big.pref[i] = pre;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = pre;
+        __syncthreads();
     }
 }
 
@@ -997,7 +1275,8 @@ int launch_geometry() {
 }
 
 // u32 scratch slots
-enum : int { kSlotN0 = 0, kSlotErr = 1, kSlotNb = 2, kSlotOut = 8, kSlotCursor = 32, kSlots = 64 };
+enum : int { kSlotN0 = 0, kSlotErr = 1, kSlotNb = 2, kSlotOver = 3, kSlotOut = 8, kSlotCursor = 32, kSlots = 64 };
+constexpr int kU64Stamp = 5;  // d_u64 slot: device clock at the start of a budgeted run
 
 }  // namespace
 
@@ -1240,29 +1519,54 @@ struct Run {
         return CUTS_OK;
     }
 
-    // The fused count of levels p and p+1 over parents [pa, pb) of L_{p-1}.
+    // The fused count of levels p and p+1 over parents [pa, pb) of L_{p-1}:
+    // phase 1 over the parents, then (counting) a scan of the parents it
+    // deferred and phase 2 over their groups.
     int launch_fused(int mode, uint32_t p, uint32_t pa, uint32_t pb) {
         CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
         const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_blocks[mode]),
                                                                          (pb - pa + kZW - 1) / kZW));
+        FusedBig fb;
+        fb.n = reinterpret_cast<unsigned long long *>(hp->fuse_big);
+        fb.cap = hp->fuse_big_cap;
+        fb.gi = hp->fuse_big + 64;
+        fb.soff = fb.gi + fb.cap;
+        fb.ns = fb.soff + fb.cap;
+        fb.pref = fb.ns + fb.cap;
+        fb.pool = fb.pref + fb.cap;
+        fb.pool_words = hp->fuse_pool_words;
+        if (mode == kCountMode) CK(cudaMemsetAsync(fb.n, 0, 2 * sizeof(unsigned long long), g.stream));
+        // CUTS_FUSE_SPLIT=<n> sets the deferral threshold (tests use small values)
+        uint32_t split = kBigS;
+        if (const char *e = std::getenv("CUTS_FUSE_SPLIT")) split = uint32_t(std::strtoul(e, nullptr, 10));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile) {
             CK(cudaEventCreate(&e0));
             CK(cudaEventCreate(&e1));
             CK(cudaEventRecord(e0, g.stream));
         }
-        if (mode == kBytesMode)
-            k_fused<kBytesMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, g.d_u64 + 2, nullptr, nullptr);
-        else
-            k_fused<kCountMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
-        CK(cudaGetLastError());
+        if (mode == kBytesMode) {
+            k_fused<kBytesMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
+                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr);
+            CK(cudaGetLastError());
+            res.launches++;
+        } else {
+            k_fused<kCountMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
+                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
+            CK(cudaGetLastError());
+            k_fused_scan<<<1, 1024, 0, g.stream>>>(fb);
+            CK(cudaGetLastError());
+            CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
+            k_fused<kCountMode><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
+                view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64,
+                g.d_u64 + 3, g.d_u64 + 4);
+            CK(cudaGetLastError());
+            res.launches += 3;
+        }
         if (profile) {
             CK(cudaEventRecord(e1, g.stream));
             marks.push_back({kCountMode, {e0, e1}});
         }
-        res.launches++;
         return CUTS_OK;
     }
 
@@ -1306,10 +1610,11 @@ struct Run {
             res.chunks++;
             CK(cudaMemcpyAsync(g.h_u32 + kSlotOut + lvl, g.d_u32 + kSlotOut + lvl, sizeof(uint32_t),
                                cudaMemcpyDeviceToHost, g.stream));
-            CK(cudaMemcpyAsync(g.h_u32 + kSlotErr, g.d_u32 + kSlotErr, sizeof(uint32_t),
+            CK(cudaMemcpyAsync(g.h_u32 + kSlotErr, g.d_u32 + kSlotErr, 3 * sizeof(uint32_t),
                                cudaMemcpyDeviceToHost, g.stream));
             rc = sync();
             if (rc) return rc;
+            if (g.h_u32[kSlotOver]) return set_error(CUTS_ERR_BUDGET, "time budget exhausted");
             const uint32_t nout = g.h_u32[kSlotOut + lvl];
             if (g.h_u32[kSlotErr] || nout > cap)
                 return set_error(CUTS_ERR_CAPACITY, "level " + std::to_string(lvl) + " overflowed its capacity");
@@ -1383,17 +1688,28 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     const uint64_t n = g.n;
     const uint64_t l0_bytes = ((8 * n + 255) / 256) * 256 + 256;
     // fused kernel: one scratch row per resident warp, as long as the longest list
-    uint64_t fuse_bytes = 0;
+    uint64_t fuse_bytes = 0, big_bytes = 0;
     if (fuse) {
         hp->fuse_stride = ((std::max<uint32_t>(g.max_deg, 1) + 31) / 32) * 32;
         fuse_bytes = uint64_t(g_fused_blocks[kCountMode] > g_fused_blocks[kBytesMode] ? g_fused_blocks[kCountMode]
                                                                                       : g_fused_blocks[kBytesMode]) *
                      kZW * hp->fuse_stride * 4;
+        // deferred parents: 256 B of counters, four arrays of cap words and a
+        // pool of saved candidate sets (1/32 of the arena, 1M..16M words)
+        hp->fuse_big_cap = 1u << 17;
+        const uint64_t pool = std::min<uint64_t>(16ull << 20, std::max<uint64_t>(1ull << 20, g.arena_bytes / 128));
+        hp->fuse_pool_words = uint32_t(std::max<uint64_t>(pool, 2ull * hp->fuse_stride));
+        big_bytes = 256 + 16ull * hp->fuse_big_cap + 4ull * hp->fuse_pool_words;
+        big_bytes = (big_bytes + 255) / 256 * 256;
+        fuse_bytes += big_bytes;
     }
     cap = 0;
     if (g.arena_bytes < l0_bytes + fuse_bytes)
         return set_error(CUTS_ERR_NOMEM, "arena smaller than the root level and scratch");
-    if (fuse) hp->fuse_scratch = reinterpret_cast<uint32_t *>(static_cast<char *>(g.arena) + g.arena_bytes - fuse_bytes);
+    if (fuse) {
+        hp->fuse_scratch = reinterpret_cast<uint32_t *>(static_cast<char *>(g.arena) + g.arena_bytes - fuse_bytes);
+        hp->fuse_big = reinterpret_cast<uint32_t *>(static_cast<char *>(g.arena) + g.arena_bytes - big_bytes);
+    }
     if (stored >= 2) {
         cap = (g.arena_bytes - l0_bytes - fuse_bytes) / (12ull * (stored - 1));
         cap = std::min<uint64_t>(cap, (1ull << 31) - 64);
@@ -1412,6 +1728,9 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
         hp->par[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
         hp->ub[i] = reinterpret_cast<uint32_t *>(cur); cur += 4 * cap;
     }
+    hp->budget_ns = 0;
+    hp->stamp = g.d_u64 + kU64Stamp;
+    hp->over = g.d_u32 + kSlotOver;
     dp = static_cast<RunParams *>(g.d_plan);
     CK(cudaMemcpyAsync(dp, hp, sizeof(RunParams), cudaMemcpyHostToDevice, g.stream));
     return CUTS_OK;
@@ -1510,6 +1829,10 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
     run.profile = opt.profile;
     run.budget_ms = opt.budget_ms;
+    if (opt.budget_ms > 0) {  // the kernels' own deadline (device time from k_roots)
+        hp->budget_ns = (unsigned long long)(opt.budget_ms * 1e6);
+        CK(cudaMemcpyAsync(dp, hp, sizeof(RunParams), cudaMemcpyHostToDevice, g.stream));
+    }
     CK(cudaEventRecord(g.ev0, g.stream));
     uint32_t n0 = 0;
     rc = run_roots(g, run, opt.shard, opt.nshards, n0);
@@ -1521,10 +1844,13 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     }
     CK(cudaEventRecord(g.ev1, g.stream));
     CK(cudaMemcpyAsync(g.h_u64, g.d_u64, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(g.h_u32 + kSlotOver, g.d_u32 + kSlotOver, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       g.stream));
     rc = run.sync();
     if (rc) return rc;
     run.collect_profile();
     CK(cudaEventElapsedTime(&res.ms, g.ev0, g.ev1));
+    if (g.h_u32[kSlotOver]) return set_error(CUTS_ERR_BUDGET, "time budget exhausted");
     const uint64_t raw = k >= 2 ? uint64_t(g.h_u64[0]) : 0;
     res.level_sizes[k - 1] = k >= 2 ? raw : n0;
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
@@ -1542,6 +1868,10 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     if (opt.want_bytes && k >= 2 && n0 > 0) {
         // untimed second pass: algorithmic bytes of the last-level kernel
         CountResult tmp;
+        if (hp->budget_ns) {  // the bytes pass runs to the end
+            hp->budget_ns = 0;
+            CK(cudaMemcpyAsync(dp, hp, sizeof(RunParams), cudaMemcpyHostToDevice, g.stream));
+        }
         Run r2{g, run.view, hp, dp, k, cap, 4, true, tmp};
         CK(cudaMemsetAsync(g.d_u64 + 2, 0, sizeof(unsigned long long), g.stream));
         rc = run_slices(r2, n0, opt.chunks);

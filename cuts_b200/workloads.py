@@ -57,72 +57,105 @@ def graph(name: str) -> "cb.HostGraph":
     raise ValueError(name)
 
 
-def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0):
-    """Score order, one query at a time, each under budget_ms."""
+def _log(*a):
+    import sys
+    print(*a, file=sys.stderr, flush=True)
+
+
+def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0, orders=None, tag="plain"):
+    """One query at a time through the level engine, each under budget_ms
+    (host check between chunks, device deadline inside the kernels); the
+    score order unless `orders` gives one per query."""
     res = []
     t0 = time.perf_counter()
-    for k, arcs in queries:
+    for i, (k, arcs) in enumerate(queries):
         q = cb.Query.from_arcs(k, arcs)
+        if orders is not None:
+            q.set_order(orders[i])
         r, done = g.count_budget(q, budget_ms, flags=flags)
         res.append((done, r.count if done else None, r.ms))
+        if (i + 1) % 50 == 0:
+            _log(f"{tag}: {i + 1}/{len(queries)} queries, {sum(d for d, _, _ in res)} finished, "
+                 f"{time.perf_counter() - t0:.1f} s")
     return res, time.perf_counter() - t0
 
 
 def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1024,
-                epochs: int = 400, seed: int = 10000, time_budget_s: float = 300.0,
+                epochs: int = 400, seed: int = 10000, time_budget_s: float = 180.0,
                 run_budget_ms: float = 100.0):
     train_q = eval_queries(n_train, seed0=seed)
     t0 = time.perf_counter()
     samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
                         time_budget_s=time_budget_s, run_budget_ms=run_budget_ms)
     t_collect = time.perf_counter() - t0
+    _log(f"training data: {len(samples)} runs in {t_collect:.1f} s")
     X, y, _ = L.features(g, train_q, samples)
     t1 = time.perf_counter()
     model = L.train(X, y, epochs=epochs, batch=4096, lr=2e-3)
     t_train = time.perf_counter() - t1
-    return model, {"samples": len(samples), "rows": int(len(y)), "collect_s": t_collect,
-                   "train_s": t_train, "fit_mae_nats": L.prediction_error(model, X, y)}
+    info = {"samples": len(samples), "queries_logged": len({s.query for s in samples}),
+            "rows": int(len(y)), "collect_s": t_collect, "train_s": t_train,
+            "fit_mae_nats": L.prediction_error(model, X, y)}
+    _log(f"model: {info}")
+    return model, info
 
 
-def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 5000.0,
-                model=None, train_budget_s: float = 600.0, flags: int = 0):
-    """Plain (score order, one query at a time) vs learned order + one batched
-    launch on the same 200 queries, both under the same per-query budget
-    (the batched launch gets budget_ms x n_eval in total)."""
+def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 1000.0,
+                model=None, train_budget_s: float = 180.0, flags: int = 0):
+    """The 200 evaluation queries three ways, each query under the same
+    budget of budget_ms of the whole GPU:
+      plain    -- score order, level engine, one query at a time;
+      learned  -- the learned order, level engine, one query at a time;
+      learned_batched -- the learned order, all queries in one persistent
+                  launch (cheapest predicted first), each limited to
+                  budget_ms of GPU time by the batched kernel's per-query limit.
+    queries/s = finished queries / seconds (planning included)."""
     info = {}
     if model is None:
         model, info = train_model(g, n_train=n_train, time_budget_s=train_budget_s)
     qdefs = eval_queries(n_eval)
     plain, plain_s = plain_pass(g, qdefs, budget_ms, flags)
     t0 = time.perf_counter()
-    qs, works = [], []
+    qs, works, orders = [], [], []
     switched = 0
     for k, arcs in qdefs:
         q = cb.Query.from_arcs(k, arcs)
-        _, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, beam=256)
+        order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, beam=256)
         switched += pw < sw
         qs.append(q)
         works.append(pw)
-    # cheapest predicted work first, so the launch budget cuts only the costliest
-    rank = sorted(range(n_eval), key=lambda i: works[i])
+        orders.append(order)
     plan_s = time.perf_counter() - t0
+    _log(f"planned {n_eval} queries in {plan_s:.1f} s, {switched} orders changed")
+    learned, learned_s = plain_pass(g, qdefs, budget_ms, flags, orders=orders, tag="learned")
+    # cheapest predicted work first
+    rank = sorted(range(n_eval), key=lambda i: works[i])
     b = g.batch([qs[i] for i in rank], flags=flags)
+    b.set_query_budget(budget_ms)
+    t1 = time.perf_counter()
     counts_r, status_r, ms = b.run(budget_ms * n_eval)
+    batch_wall = time.perf_counter() - t1
     counts = [0] * n_eval
     status = [0] * n_eval
     for j, i in enumerate(rank):
         counts[i], status[i] = counts_r[j], status_r[j]
-    learned_s = plan_s + ms / 1e3
+    lb_s = plan_s + batch_wall
     done_p = [d for d, _, _ in plain]
-    done_l = [s == 0 for s in status]
+    done_l = [d for d, _, _ in learned]
+    done_b = [s == 0 for s in status]
     agree = all(c == pc for (d, pc, _), c, s in zip(plain, counts, status) if d and s == 0)
+    agree = agree and all(lc == pc for (d, pc, _), (dl, lc, _) in zip(plain, learned) if d and dl)
+    fin_k = lambda done: {k: sum(1 for (kk, _), d in zip(qdefs, done) if d and kk == k) for k in range(5, 9)}
     return {
         "queries": n_eval, "budget_ms_per_query": budget_ms,
         "plain": {"finished": sum(done_p), "seconds": plain_s,
-                  "queries_per_s": sum(done_p) / plain_s},
-        "learned_batched": {"finished": sum(done_l), "seconds": learned_s, "plan_s": plan_s,
-                            "launch_ms": ms, "queries_per_s": sum(done_l) / learned_s,
-                            "orders_changed": switched},
+                  "queries_per_s": sum(done_p) / plain_s, "finished_by_k": fin_k(done_p)},
+        "learned": {"finished": sum(done_l), "seconds": plan_s + learned_s, "plan_s": plan_s,
+                    "queries_per_s": sum(done_l) / (plan_s + learned_s), "orders_changed": switched,
+                    "finished_by_k": fin_k(done_l)},
+        "learned_batched": {"finished": sum(done_b), "seconds": lb_s, "plan_s": plan_s,
+                            "launch_ms": ms, "launch_wall_s": batch_wall,
+                            "queries_per_s": sum(done_b) / lb_s, "finished_by_k": fin_k(done_b)},
         "counts_agree_where_both_finished": agree,
         "training": info,
     }
@@ -140,10 +173,10 @@ def stripe_estimates(g: "cb.Graph", qs, stride: int = 1 << 16, budget_ms: float 
 
 
 def run_batched(g: "cb.Graph", n: int = 4096, budget_ms: float = 60000.0, tune_sample: int = 256,
-                flags: int = 0):
-    """4,096 queries in one persistent launch, cheapest estimated first (so
-    the device-time budget cuts only the costliest); shape autotuned on a
-    sample."""
+                flags: int = 0, query_budget_ms: float = 50.0):
+    """4,096 queries in one persistent launch, cheapest estimated first, each
+    limited to query_budget_ms of the whole GPU and the launch to budget_ms;
+    shape autotuned on a sample."""
     from cuts_b200 import autotune
     qdefs = batched_queries(n)
     qs0 = [cb.Query.from_arcs(k, a) for k, a in qdefs]
@@ -153,12 +186,16 @@ def run_batched(g: "cb.Graph", n: int = 4096, budget_ms: float = 60000.0, tune_s
     qs = [qs0[i] for i in rank]
     est_s = time.perf_counter() - t_est
     t0 = time.perf_counter()
-    best, times = autotune.tune_batch(g, qs[:tune_sample], flags=flags, budget_ms=2000.0)
+    best, times = autotune.tune_batch(g, qs[:tune_sample], flags=flags, budget_ms=2000.0,
+                                      query_budget_ms=query_budget_ms)
     tune_s = time.perf_counter() - t0
     b = g.batch(qs, flags=flags, grain=best[0], tasks_per_grab=best[1], blocks_per_sm=best[2])
+    b.set_query_budget(query_budget_ms)
+    _log(f"batched: estimates {est_s:.1f} s, tuned {best} in {tune_s:.1f} s")
     counts, status, ms = b.run(budget_ms)
     fin = sum(1 for s in status if s == 0)
     return {"queries": n, "finished": fin, "launch_ms": ms, "queries_per_s": fin / (ms / 1e3),
+            "query_budget_ms": query_budget_ms, "launch_budget_ms": budget_ms,
             "tuned": list(best), "tune_s": tune_s, "estimate_s": est_s, "tasks": b.info()[0],
             "matches_finished": int(sum(c for c, s in zip(counts, status) if s == 0)),
             "finished_by_k": {k: sum(1 for i, s in zip(rank, status) if s == 0 and qdefs[i][0] == k)

@@ -187,8 +187,11 @@ int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t fla
                        uint32_t shard, uint32_t nshards, uint64_t *count, float *ms,
                        uint64_t *level_sizes);
 
-/* As cuts_count, but stops with CUTS_ERR_BUDGET once budget_ms of host time
- * has passed (checked between chunks; the running chunk completes). */
+/* As cuts_count, but stops with CUTS_ERR_BUDGET once budget_ms has passed:
+ * the host checks between chunks, and every kernel of the run stops taking
+ * work once budget_ms of device time has passed since the run's first
+ * kernel, so one oversized chunk cannot overrun the budget by more than the
+ * work items already in flight. */
 int cuts_count_budget(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
                       double budget_ms, uint64_t *count, float *ms, uint64_t *level_sizes);
 
@@ -268,6 +271,12 @@ int cuts_batch_create(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t 
  * device time of the launch. */
 int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status, float *ms);
 /* tasks in the launch, launch blocks */
+/* Per-query limit for later cuts_batch_run calls: each query may use ms of
+ * the whole GPU (its warp time summed over the launch's warps, up to ms x the
+ * launch's warps); a query past it reports CUTS_ERR_BUDGET while the others
+ * carry on.  0 = no limit (the default).  No reference counterpart: the
+ * reference runs one query per process. */
+int cuts_batch_set_query_budget(cuts_batch b, double ms);
 int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks);
 void cuts_batch_free(cuts_batch b);
 

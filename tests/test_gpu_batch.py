@@ -115,3 +115,44 @@ def test_level_engine_budget():
     g.set_level_cap(0)
     r, done = g.count_budget(q, 0.0)
     assert done and r.count == g.count(q).count
+
+
+def test_level_engine_device_budget():
+    """One large chunk: the kernels' own deadline stops the run well before
+    the work would end (the host check between chunks never runs)."""
+    import time
+    h = cb.HostGraph.chung_lu(20000, 80000, 2.1, 2.0, 2000.0, seed=9)
+    g = h.upload(0)
+    q = cb.Query.from_arcs(*cb.named_query_arcs("6-cycle"))
+    sample, sdone = g.count_sample(q, 0, 64, budget_ms=5000.0)
+    full_est_ms = sample.ms * 64 if sdone else 5000.0 * 64
+    assert full_est_ms > 200  # the whole count takes far longer than the budget
+    t = time.perf_counter()
+    r, done = g.count_budget(q, 20.0, chunks=1)
+    wall = time.perf_counter() - t
+    assert not done
+    assert wall < 0.5 * full_est_ms / 1e3 + 0.1
+    # a budget the run fits in: exact (a root stripe, to stay short)
+    if sdone:
+        r2, done2 = g.count_sample(q, 0, 64, budget_ms=1e7)
+        assert done2 and r2.count == sample.count
+
+
+def test_batch_query_budget_drops_only_the_heavy_query():
+    """A per-query limit: the heavy query placed first is dropped once it has
+    used its share, the cheap ones behind it finish with exact counts."""
+    h = cb.HostGraph.chung_lu(20000, 80000, 2.1, 2.0, 2000.0, seed=9)
+    g = h.upload(0)
+    heavy = cb.Query.from_arcs(*cb.named_query_arcs("6-cycle"))
+    cheap = [cb.Query.from_arcs(*cb.named_query_arcs(n)) for n in ("triangle", "4-cycle", "triangle")]
+    b = g.batch([heavy] + cheap)
+    b.set_query_budget(5.0)
+    counts, status, ms = b.run()
+    assert status[0] == cb.ERR_BUDGET
+    assert status[1:] == [0, 0, 0]
+    for c, q in zip(counts[1:], cheap):
+        assert c == g.count(q).count
+    b.set_query_budget(0.0)
+    b2 = g.batch(cheap)
+    c2, s2, _ = b2.run()
+    assert s2 == [0, 0, 0] and c2 == counts[1:]

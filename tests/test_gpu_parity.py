@@ -293,3 +293,53 @@ def test_fused_with_forced_chunking(cl5k):
         assert r.count == cnt and r.level_sizes == lv
     finally:
         g.set_level_cap(0)
+
+
+@pytest.mark.parametrize("split", ["0", "1", "7", "40"])
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK])
+def test_fused_split_parents(er2k, cl5k, monkeypatch, split, flags):
+    """Parents whose candidate set exceeds the split threshold are deferred to
+    the second phase (groups of 32 vertices spread over all warps); with small
+    thresholds nearly every parent goes there, and with threshold 0 on the
+    power-law graph the saved-set pool runs out, so the in-place fallback is
+    taken too.  Counts and level sizes against the oracle."""
+    monkeypatch.setenv("CUTS_FUSE_SPLIT", split)
+    for name in ("triangle", "4-clique", "4-clique+pendant", "diamond", "house"):
+        k, arcs = FUSE_QUERIES[name]
+        for h, g, od in (er2k, cl5k):
+            q = cb.Query.from_arcs(k, arcs)
+            cnt, lv, _ = oracle_count(od, k, arcs, q.order)
+            r = g.count(q, flags=flags, stats=True)
+            assert r.count == cnt, (name, split)
+            if flags == 0:
+                assert r.level_sizes == lv, (name, split)
+
+
+def test_fused_split_directed(monkeypatch):
+    monkeypatch.setenv("CUTS_FUSE_SPLIT", "3")
+    n, src, dst = directed_er(1500, 14.0, seed=11)
+    oo, oa, io, ia, s_, d_ = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo, oa, io, ia)
+    od = O.Graph.from_arrays(n, s_, d_)
+    for name in ("directed-triangle-mixed", "directed-4-clique"):
+        k, arcs = FUSE_QUERIES[name]
+        q = cb.Query.from_arcs(k, arcs)
+        cnt, lv, _ = oracle_count(od, k, arcs, q.order)
+        r = g.count(q, stats=True)
+        assert r.count == cnt and r.level_sizes == lv
+
+
+def test_fused_hub_graph_matches_unfused():
+    """A graph with hubs of degree > 256 (the default split threshold): the
+    fused plan, with its deferred hub parents, against the unfused plan."""
+    h = cb.HostGraph.chung_lu(20000, 80000, 2.1, 2.0, 2000.0, seed=9)
+    g = h.upload(0)
+    assert h.info()[3] > 256
+    for name in ("triangle", "4-clique", "4-clique+pendant", "diamond"):
+        k, arcs = FUSE_QUERIES[name]
+        q = cb.Query.from_arcs(k, arcs)
+        for flags in (0, cb.FLAG_SYMMETRY_BREAK):
+            a = g.count(q, flags=flags, stats=True)
+            b = g.count(q, flags=flags | cb.FLAG_NO_FUSE, stats=True)
+            assert a.count == b.count, (name, flags)
+            assert a.level_sizes == b.level_sizes, (name, flags)
