@@ -417,8 +417,15 @@ def main():
         ll_ms, ll_n, ll_bytes = kern["last_level"]
         achieved = (ll_bytes / max(ll_n, 1)) / ((ll_ms / max(ll_n, 1)) / 1e3) / 1e9 if ll_ms else None
         traffic = ncu_traffic().get("last_level_bytes_per_launch")
+        # the counting kernel of each query: fused with the level before, or flat
+        sym = h.info()[2]
+        kinds = []
+        for name, q in queries:
+            lv, _ = q.plan_levels(sym, args.flags)
+            fused = any(x["fuse"] for x in lv) and os.environ.get("CUTS_NO_FUSE") != "1"
+            kinds.append(f"{'k_fused' if fused else 'k_level_flat'}<count> ({name})")
         roofline = {
-            "kernel": "k_level_flat<count> (last counted trie level)",
+            "kernel": "last counted level: " + ", ".join(kinds),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
             "peak_source": peak_kind,

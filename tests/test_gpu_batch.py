@@ -143,10 +143,12 @@ def test_batch_query_budget_drops_only_the_heavy_query():
     used its share, the cheap ones behind it finish with exact counts."""
     h = cb.HostGraph.chung_lu(20000, 80000, 2.1, 2.0, 2000.0, seed=9)
     g = h.upload(0)
-    heavy = cb.Query.from_arcs(*cb.named_query_arcs("6-cycle"))
-    cheap = [cb.Query.from_arcs(*cb.named_query_arcs(n)) for n in ("triangle", "4-cycle", "triangle")]
+    # a 7-vertex path: ~1e15 embeddings around the degree-2,000 hubs
+    path7 = [(a, b) for i in range(6) for a, b in ((i, i + 1), (i + 1, i))]
+    heavy = cb.Query.from_arcs(7, path7)
+    cheap = [cb.Query.from_arcs(*cb.named_query_arcs(n)) for n in ("triangle", "4-clique+pendant", "triangle")]
     b = g.batch([heavy] + cheap)
-    b.set_query_budget(5.0)
+    b.set_query_budget(200.0)
     counts, status, ms = b.run()
     assert status[0] == cb.ERR_BUDGET
     assert status[1:] == [0, 0, 0]
