@@ -33,6 +33,7 @@ MAX_QUERY = 16
 FLAG_SYMMETRY_BREAK = 1
 FLAG_NO_CLOSED_FORM = 2
 FLAG_NO_FUSE = 4
+FLAG_NO_ORBIT_FOLD = 8
 ORDER_SCORE = 0
 ORDER_LEARNED = 1
 
@@ -302,14 +303,15 @@ class Query:
         return [int(x) for x in o], pw.value, sw.value
 
     def plan_levels(self, data_symmetric: bool = True, flags: int = 0):
-        """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt) and |Aut| used."""
+        """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt, fuse,
+        ofold) and the count multiplier used."""
         k = self.k
-        out = np.zeros(8 * k, np.uint32)
+        out = np.zeros(9 * k, np.uint32)
         aut = C.c_uint64()
         _check(lib().cuts_query_plan_levels(self._h, int(data_symmetric), flags, _ptr(out, _u32p),
                                             C.byref(aut)))
-        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse"]
-        return [dict(zip(keys, (int(x) for x in out[8 * i:8 * i + 8]))) for i in range(k)], aut.value
+        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse", "ofold"]
+        return [dict(zip(keys, (int(x) for x in out[9 * i:9 * i + 9]))) for i in range(k)], aut.value
 
     def automorphisms(self) -> int:
         a = C.c_uint64()

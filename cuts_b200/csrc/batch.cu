@@ -431,7 +431,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
     for (uint32_t i = 0; i < nq; ++i) {
         const Query &q = *qs[i];
         Plan plan;
-        rc = build_plan(q, g->symmetric, flags, plan);
+        rc = build_plan(q, g->symmetric, flags | CUTS_FLAG_NO_ORBIT_FOLD, plan);  // plain fold only
         if (rc) return rc;
         aut[i] = plan.aut;
         BQuery b;
@@ -685,7 +685,7 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
         if (q.k > uint32_t(kBatchMaxK))
             return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: query with more than 10 vertices");
         Plan plan;
-        int rc = build_plan(q, sym, flags, plan);
+        int rc = build_plan(q, sym, flags | CUTS_FLAG_NO_ORBIT_FOLD, plan);  // plain fold only
         if (rc) return rc;
         BQuery &b = table[i];
         std::memset(&b, 0, sizeof(b));

@@ -84,6 +84,39 @@ __device__ __forceinline__ bool past_deadline(const RunParams *rp, unsigned long
     return true;
 }
 
+// Orbit fold (a pendant's closed form summed over its attachment orbit O):
+// the part of the weight fixed by positions below `upto`,
+//   sum_{x in O, x < upto} ( |L(m_x)| - #{j < upto : m_j in L(m_x)} ),
+// where m(j) gives the matched vertex of position j.
+template <class M>
+__device__ __forceinline__ uint32_t orbit_base(const DevView &g, const LevelPlan &F, uint32_t upto, M m) {
+    uint32_t base = 0;
+    for (uint32_t xm = F.ofold & ((1u << upto) - 1); xm; xm &= xm - 1) {
+        const uint32_t x = __ffs(xm) - 1;
+        const uint2 inf = F.jdir[0] ? g.in_info[m(x)] : g.out_info[m(x)];
+        const uint32_t *l = g.adj + inf.x;
+        uint32_t sub = 0;
+        for (uint32_t j = 0; j < upto; ++j)
+            if (((F.oguar[x] >> j) & 1u) || contains(l, inf.y, m(j))) ++sub;
+        base += inf.y - sub;
+    }
+    return base;
+}
+
+// The weight of candidate t at position c given the base of positions below
+// c: each earlier orbit list holds t (implied by the query's arcs, checked at
+// plan time), and when c is in the orbit, t's own list holds every m_j, j < c.
+__device__ __forceinline__ uint32_t orbit_weight(const DevView &g, const LevelPlan &F, uint32_t c,
+                                                 uint32_t base, uint32_t t, bool loops) {
+    uint32_t w = base - __popc(F.ofold & ((1u << c) - 1));
+    if ((F.ofold >> c) & 1u) {
+        const uint2 ti = F.jdir[0] ? g.in_info[t] : g.out_info[t];
+        w += ti.y - c;
+        if (loops && contains(g.adj + ti.x, ti.y, t)) --w;
+    }
+    return w;
+}
+
 enum Mode { kExpand = 0, kCountMode = 1, kBytesMode = 2 };
 
 // ---- level 0: signature scan (device_funcs.cu:267-279) ---------------
@@ -408,6 +441,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     // is an earlier vertex's list and c itself is one of the matched
     const bool fold = MODE != kExpand && sL.fold;
     const bool fold_guar_c = fold && ((sN.guar_mask >> lvl) & 1u);
+    const bool loops = rp->plan.data_loops != 0;
     const uint32_t total = pb - pa;
     const unsigned long long deadline = run_deadline(rp);
     unsigned long long local = 0, local2 = 0;
@@ -475,7 +509,9 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                         const uint32_t u = sm_m[warp][sN.jpos[t]][lane];
                         ubp = min(ubp, (sN.jdir[t] ? g.in_info[u] : g.out_info[u]).y);
                     }
-            if (fold) {
+            if (fold && sN.ofold) {
+                fbase = orbit_base(g, sN, lvl, [&](uint32_t j) { return sm_m[warp][j][lane]; });
+            } else if (fold) {
                 const uint32_t u = sm_m[warp][sN.jpos[0]][lane];
                 const uint2 inf = sN.jdir[0] ? g.in_info[u] : g.out_info[u];
                 f_off = inf.x;
@@ -593,7 +629,10 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                     const uint32_t o_fdeg = __shfl_sync(kFullMask, f_deg, int(owner));
                     const uint32_t o_flo = __shfl_sync(kFullMask, f_lo, int(owner));
                     const uint32_t o_fhi = __shfl_sync(kFullMask, f_hi, int(owner));
-                    if (ok) {
+                    if (ok && sN.ofold) {
+                        local += orbit_weight(g, sN, lvl, o_fbase, c, loops);
+                        ++local2;
+                    } else if (ok) {
                         const bool hit = c >= o_flo && c < o_fhi &&
                                          (fold_guar_c || contains(g.adj + o_foff, o_fdeg, c));
                         local += o_fbase - (hit ? 1u : 0u);
@@ -706,6 +745,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
     const uint32_t below = (1u << p) - 1;
     const bool c_gt_s = (sC.gt_mask >> p) & 1u, c_lt_s = (sC.lt_mask >> p) & 1u;
     const bool fguar_t = cfold && ((sF.guar_mask >> c) & 1u);
+    const bool loops = rp->plan.data_loops != 0;
     // an extra list of c on position p itself changes with s: per-s loop
     bool extra_on_p = false;
     for (uint32_t t = 0; t < sC.nj; ++t)
@@ -752,7 +792,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 ooff = iters ? lsoff : 0;
                 ostart = iters ? ls0 : ts;
                 oend = iters ? ls1 : te;
-                if (cfold) {
+                if (cfold && sF.ofold) {
+                    fbase = orbit_base(g, sF, p + 1, [&](uint32_t j) { return j == p ? sv : my_m[j]; });
+                } else if (cfold) {
                     // folded last level: f_base(s) = |window of L_F| - matched in it
                     const uint32_t jf = sF.jpos[0];
                     const uint32_t u = jf == p ? sv : my_m[jf];
@@ -848,7 +890,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 }
                 if (ok) {
                     ++local_c;
-                    if (cfold) {
+                    if (cfold && sF.ofold) {
+                        local += orbit_weight(g, sF, c, o_fbase, t, loops);
+                    } else if (cfold) {
                         const bool h = t >= o_flo && t < o_fhi && (fguar_t || contains(g.adj + o_foff, o_fdeg, t));
                         local += o_fbase - (h ? 1u : 0u);
                     } else {
@@ -880,7 +924,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             }
             uint32_t fbase = 0, fdeg = 0, flo = 0, fhi = kFullMask;
             const uint32_t *fl = nullptr;
-            if (cfold) {
+            if (cfold && sF.ofold) {
+                fbase = orbit_base(g, sF, p + 1, [&](uint32_t j) { return j == p ? sv : my_m[j]; });
+            } else if (cfold) {
                 const uint32_t jf = sF.jpos[0];
                 const uint32_t u = jf == p ? sv : my_m[jf];
                 const uint2 inf = sF.jdir[0] ? g.in_info[u] : g.out_info[u];
@@ -944,7 +990,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 }
                 if (ok) {
                     ++local_c;
-                    if (cfold) {
+                    if (cfold && sF.ofold) {
+                        local += orbit_weight(g, sF, c, fbase, t, loops);
+                    } else if (cfold) {
                         const bool h = t >= flo && t < fhi && (fguar_t || contains(fl, fdeg, t));
                         local += fbase - (h ? 1u : 0u);
                     } else {
@@ -1319,6 +1367,15 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     g->arcs = hg.arcs;
     g->symmetric = hg.symmetric;
     g->max_deg = hg.max_degree();
+    {
+        bool loops = false;
+        #pragma omp parallel for reduction(|| : loops) schedule(static)
+        for (int64_t v = 0; v < int64_t(n); ++v) {
+            const uint32_t *l = hg.out_list(uint32_t(v));
+            if (std::binary_search(l, l + hg.out_deg(uint32_t(v)), uint32_t(v))) loops = true;
+        }
+        g->loops = loops;
+    }
     g->adj_words = adj.size();
     g->stats = degree_stats(hg);
     g->h_out_deg.resize(n);
@@ -1661,6 +1718,21 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     int rc = build_plan(q, g.symmetric, flags, hp->plan);
     if (rc) return rc;
     const bool counting = stored == k - 1;
+    const char *nf = std::getenv("CUTS_NO_FUSE");  // 1 = fusion off process-wide (A/B comparisons)
+    const bool env_nofuse = nf && nf[0] == '1';
+    if (k >= 3 && hp->plan.lv[k - 1].ofold) {
+        // the orbit fold needs its weight evaluated by the flattened or the
+        // fused counting kernel, in 32 bits; otherwise break Q's symmetry
+        const bool fused = hp->plan.lv[k - 2].fuse && !env_nofuse;
+        const bool flat = g_use_flat && hp->plan.lv[k - 2].nj <= uint32_t(kFJ);
+        const bool fits = uint64_t(__builtin_popcount(hp->plan.lv[k - 1].ofold)) *
+                              std::max<uint32_t>(g.max_deg, 1) < (1ull << 32);
+        if (!counting || !(fused || flat) || !fits) {
+            rc = build_plan(q, g.symmetric, flags | CUTS_FLAG_NO_ORBIT_FOLD, hp->plan);
+            if (rc) return rc;
+        }
+    }
+    hp->plan.data_loops = g.loops ? 1u : 0u;
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
         // the folded count runs in the flattened or the fused kernel only
         const bool fused_here = hp->plan.lv[k - 2].fuse != 0;
@@ -1670,9 +1742,7 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     // the counted level and, when fused, the one before it are not stored
     const uint32_t cl = (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
     if (k >= 3 && !hp->plan.lv[k - 2].fold) hp->plan.lv[k - 2].fuse = 0;
-    // CUTS_NO_FUSE=1 turns fusion off process-wide (A/B comparisons)
-    const char *nf = std::getenv("CUTS_NO_FUSE");
-    if (!counting || (nf && nf[0] == '1'))
+    if (!counting || env_nofuse)
         for (uint32_t i = 0; i < k; ++i) hp->plan.lv[i].fuse = 0;
     const bool fuse = counting && k >= 3 && hp->plan.lv[cl].fuse;
     if (fuse) stored = cl - 1;

@@ -17,6 +17,7 @@ struct DeviceGraph {
     uint64_t arcs = 0;
     bool symmetric = false;
     uint32_t max_deg = 0;
+    bool loops = false;  // some vertex lists itself (a self-loop arc)
     uint2 *out_info = nullptr;
     uint2 *in_info = nullptr;
     uint32_t *adj = nullptr;

@@ -102,6 +102,10 @@ struct LevelPlan {
                               // candidate sets (see build_plan)
     uint32_t fuse_extra;      // mask of c's joins beyond c-1's joins and (c-1)
     uint32_t fuse_tp;         // index of c's join on position c-1
+    uint32_t ofold;           // last level, orbit fold: positions x of the
+                              // pendant's attachment orbit (0 = plain fold)
+    uint32_t oguar[kMaxK];    // orbit fold: positions j with m_j guaranteed
+                              // in the list of m_x, per orbit position x
     uint8_t jpos[kMaxJ];      // joined position j
     uint8_t jdir[kMaxJ];      // 0: out-list of m_j (P join), 1: in-list (C join)
 };
@@ -110,6 +114,7 @@ struct Plan {
     uint32_t k;
     uint32_t symmetric;       // data graph symmetric: in-lists == out-lists
     uint64_t aut;             // multiplier applied to the count (1 or |Aut|)
+    uint32_t data_loops;      // the data graph has self-loops (set by the engine)
     LevelPlan lv[kMaxK];
 };
 

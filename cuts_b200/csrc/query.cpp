@@ -249,6 +249,77 @@ uint64_t automorphism_count(const Query &q) {
 
 // ---- plan ---------------------------------------------------------------
 
+// Orbit fold.  When the last vertex e of the order is a pendant on vertex a
+// (its level is a closed form over a's list L), every embedding of Q is an
+// embedding psi of the core C = Q - e plus one vertex of L(psi(a)) outside
+// psi(C).  Summing over the |Aut(C)| embeddings psi = phi o sigma of one
+// class, psi(a) = phi(x) runs over the orbit O of a under Aut(C), each x
+// |Aut(C)| / |O| times, so
+//   count(Q) = |Aut(C)| / |O| x sum over one phi per class of
+//              sum_{x in O} ( |L(phi(x))| - |L(phi(x)) n phi(C)| ).
+// The core's own symmetry is broken (its stabiliser chain), which leaves
+// |O| times fewer core embeddings to enumerate than breaking Q's.  The
+// weight is evaluated at level k-2 (a fold); the memberships that involve
+// the level k-2 vertex must be implied by the query's arcs, so that the
+// per-candidate weight needs no list search.  Returns false (plan untouched)
+// when the query does not have that shape or the orbit is trivial.
+static bool orbit_fold_plan(const Query &q, bool data_symmetric, Plan &plan) {
+    const uint32_t k = q.k, c = k - 2;
+    LevelPlan &F = plan.lv[k - 1];
+    if (k < 3 || !F.closed_form || F.nj != 1) return false;
+    const uint32_t jf = F.jpos[0], dir = F.jdir[0];
+    const uint32_t e = q.order[k - 1];
+    std::vector<uint32_t> pos(k);
+    for (uint32_t i = 0; i < k; ++i) pos[q.order[i]] = i;
+    // the core, relabelled by position
+    Query C;
+    C.k = k - 1;
+    C.out.assign(k - 1, {});
+    C.in.assign(k - 1, {});
+    for (uint32_t i = 0; i + 1 < k; ++i) {
+        const uint32_t v = q.order[i];
+        for (uint32_t w : q.out[v])
+            if (w != e) C.out[i].push_back(pos[w]);
+        for (uint32_t w : q.in[v])
+            if (w != e) C.in[i].push_back(pos[w]);
+        std::sort(C.out[i].begin(), C.out[i].end());
+        std::sort(C.in[i].begin(), C.in[i].end());
+    }
+    for (uint32_t i = 0; i + 1 < k; ++i) C.order.push_back(i);
+    uint32_t omask = 1u << jf;
+    for (uint32_t x = 0; x + 1 < k; ++x)
+        if (x != jf && find_automorphism(C, {}, jf, x)) omask |= 1u << x;
+    if (__builtin_popcount(omask) < 2) return false;
+    // m_j is in the list of m_x whenever the query has the arc that list stands for
+    uint32_t oguar[kMaxK] = {};
+    for (uint32_t x = 0; x + 1 < k; ++x) {
+        if (!((omask >> x) & 1u)) continue;
+        for (uint32_t j = 0; j + 1 < k; ++j) {
+            if (j == x) continue;
+            const uint32_t a = q.order[x], b = q.order[j];
+            const bool fwd = dir == 0 ? q.has_arc(a, b) : q.has_arc(b, a);
+            const bool rev = dir == 0 ? q.has_arc(b, a) : q.has_arc(a, b);
+            if (fwd || (data_symmetric && rev)) oguar[x] |= 1u << j;
+        }
+    }
+    for (uint32_t x = 0; x < c; ++x)
+        if (((omask >> x) & 1u) && !((oguar[x] >> c) & 1u)) return false;
+    if (((omask >> c) & 1u) && (oguar[c] & ((1u << c) - 1)) != ((1u << c) - 1)) return false;
+    std::vector<std::pair<uint32_t, uint32_t>> conds;
+    uint64_t autc = 1;
+    stabiliser_chain(C, &conds, &autc);
+    for (auto &cd : conds) {  // f(a) < f(b), positions
+        const uint32_t pa = cd.first, pb = cd.second;
+        if (pb > pa) plan.lv[pb].gt_mask |= 1u << pa;
+        else plan.lv[pa].lt_mask |= 1u << pb;
+    }
+    plan.aut = autc / uint64_t(__builtin_popcount(omask));
+    F.ofold = omask;
+    for (uint32_t x = 0; x < kMaxK; ++x) F.oguar[x] = oguar[x];
+    plan.lv[k - 2].fold = 1;
+    return true;
+}
+
 int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) {
     plan = Plan();
     plan.k = q.k;
@@ -294,7 +365,9 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
             }
         }
     }
-    if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && k >= 2) {
+    const bool orbit = (flags & CUTS_FLAG_SYMMETRY_BREAK) && !(flags & CUTS_FLAG_NO_ORBIT_FOLD) &&
+                       q.loop_free() && k >= 3 && orbit_fold_plan(q, data_symmetric, plan);
+    if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && k >= 2 && !orbit) {
         std::vector<uint32_t> pos(k);
         for (uint32_t i = 0; i < k; ++i) pos[q.order[i]] = i;
         std::vector<std::pair<uint32_t, uint32_t>> conds;

@@ -80,9 +80,9 @@ def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0, orders=
     return res, time.perf_counter() - t0
 
 
-def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1024,
-                epochs: int = 400, seed: int = 10000, time_budget_s: float = 180.0,
-                run_budget_ms: float = 100.0):
+def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1 << 14,
+                epochs: int = 400, seed: int = 10000, time_budget_s: float = 120.0,
+                run_budget_ms: float = 200.0):
     train_q = eval_queries(n_train, seed0=seed)
     t0 = time.perf_counter()
     samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
@@ -100,8 +100,29 @@ def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, s
     return model, info
 
 
-def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 1000.0,
-                model=None, train_budget_s: float = 180.0, flags: int = 0):
+def estimate_orders(g: "cb.Graph", qdefs, orders_a, orders_b, stride: int, budget_ms: float,
+                    flags: int = 0):
+    """Estimated device time of a full exact count of each query under two
+    orders, from the same root stripe (u % stride == 0; the stripe's time x
+    stride); None where the stripe itself exceeds budget_ms."""
+    out = []
+    t0 = time.perf_counter()
+    for i, (k, arcs) in enumerate(qdefs):
+        row = []
+        for orders in (orders_a, orders_b):
+            q = cb.Query.from_arcs(k, arcs)
+            q.set_order(orders[i])
+            r, done = g.count_sample(q, 0, stride, budget_ms, flags)
+            row.append(r.ms * stride if done else None)
+        out.append(row)
+        if (i + 1) % 50 == 0:
+            _log(f"estimates: {i + 1}/{len(qdefs)} queries, {time.perf_counter() - t0:.1f} s")
+    return out
+
+
+def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 250.0,
+                model=None, train_budget_s: float = 120.0, flags: int = 0,
+                est_stride: int = 1 << 12, est_budget_ms: float = 300.0):
     """The 200 evaluation queries three ways, each query under the same
     budget of budget_ms of the whole GPU:
       plain    -- score order, level engine, one query at a time;
@@ -127,6 +148,24 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
         orders.append(order)
     plan_s = time.perf_counter() - t0
     _log(f"planned {n_eval} queries in {plan_s:.1f} s, {switched} orders changed")
+    score_orders = [cb.Query.from_arcs(k, arcs).order for k, arcs in qdefs]
+    est = estimate_orders(g, qdefs, score_orders, orders, est_stride, est_budget_ms, flags)
+    both = [(a, b) for a, b in est if a is not None and b is not None]
+    est_rep = {
+        "stride": est_stride, "stripe_budget_ms": est_budget_ms,
+        "queries_estimated_both": len(both),
+        "score_only": sum(1 for a, b in est if a is not None and b is None),
+        "learned_only": sum(1 for a, b in est if a is None and b is not None),
+        "sum_est_s_score": sum(a for a, _ in both) / 1e3,
+        "sum_est_s_learned": sum(b for _, b in both) / 1e3,
+        "geomean_speedup": (math.exp(sum(math.log(max(a, 1e-3) / max(b, 1e-3)) for a, b in both) / len(both))
+                            if both else None),
+        "learned_faster": sum(1 for a, b in both if b < a * 0.9),
+        "learned_slower": sum(1 for a, b in both if b > a * 1.1),
+        "est_full_s_quantiles_score": ([float(x) for x in np.quantile([a / 1e3 for a, _ in both],
+                                                                       [0.1, 0.5, 0.9])] if both else None),
+    }
+    _log(f"estimates: {est_rep}")
     learned, learned_s = plain_pass(g, qdefs, budget_ms, flags, orders=orders, tag="learned")
     # cheapest predicted work first
     rank = sorted(range(n_eval), key=lambda i: works[i])
@@ -157,6 +196,7 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
                             "launch_ms": ms, "launch_wall_s": batch_wall,
                             "queries_per_s": sum(done_b) / lb_s, "finished_by_k": fin_k(done_b)},
         "counts_agree_where_both_finished": agree,
+        "estimated_full_counts": est_rep,
         "training": info,
     }
 

@@ -37,6 +37,10 @@ extern "C" {
                                         closed form exists */
 #define CUTS_FLAG_NO_FUSE 4u         /* materialise the level before the counted
                                         one even when it could be fused */
+#define CUTS_FLAG_NO_ORBIT_FOLD 8u   /* with CUTS_FLAG_SYMMETRY_BREAK: break the
+                                        whole query's symmetry even when the last
+                                        vertex is a pendant whose removal leaves
+                                        a more symmetric core */
 
 /* order modes for cuts_plan */
 #define CUTS_ORDER_SCORE 0    /* greedy score order (score.cpp) */
@@ -140,10 +144,10 @@ int cuts_query_joins(cuts_query q, uint32_t *p_off, uint32_t *p, uint32_t *c_off
 int cuts_query_set_order(cuts_query q, const uint32_t *order);
 
 /* The per-level plan the kernels run for the current order, for a data
- * graph that is symmetric or not and the given flags: 8 words per level,
+ * graph that is symmetric or not and the given flags: 9 words per level,
  * {joined lists, signature test, closed form, folded into the level before,
  * guaranteed-member mask, greater-than mask, less-than mask, fused with the
- * level before}.  Host only;
+ * level before, orbit-fold positions}.  Host only;
  * no reference counterpart (the reference derives joins per launch,
  * device_funcs.cu:103-127). */
 int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,

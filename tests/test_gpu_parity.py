@@ -343,3 +343,51 @@ def test_fused_hub_graph_matches_unfused():
             b = g.count(q, flags=flags | cb.FLAG_NO_FUSE, stats=True)
             assert a.count == b.count, (name, flags)
             assert a.level_sizes == b.level_sizes, (name, flags)
+
+
+ORBIT_QUERIES = {
+    "4-clique+pendant": cb.named_query_arcs("4-clique+pendant"),
+    "5-clique+pendant": (6, [(a, b) for a in range(6) for b in range(6)
+                             if a != b and (a < 5 and b < 5 or {a, b} == {0, 5})]),
+    "paw": (4, [(0, 1), (1, 0), (1, 2), (2, 1), (0, 2), (2, 0), (0, 3), (3, 0)]),
+    "diamond+pendant": (5, [(a, b) for u, v in [(0, 1), (0, 2), (1, 2), (1, 3), (2, 3), (1, 4)]
+                            for a, b in ((u, v), (v, u))]),
+    "dir3cycle+pendant": (4, [(0, 1), (1, 2), (2, 0), (0, 3)]),
+}
+
+
+@pytest.fixture(scope="module")
+def loops_graph():
+    """Symmetric ER graph with a self-loop on every third vertex."""
+    n = 200
+    h = cb.HostGraph.erdos_renyi(n, 0.15, seed=4)
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(oo.astype(np.int64)))
+    loops = np.arange(0, n, 3, dtype=np.uint32)
+    src = np.concatenate([src, loops])
+    dst = np.concatenate([oa, loops])
+    oo2, oa2, io2, ia2, s, d = csr_from_arcs(n, src, dst)
+    return None, cb.Graph.from_csr(n, oo2, oa2, io2, ia2), O.Graph.from_arrays(n, s, d)
+
+
+@pytest.mark.parametrize("name", sorted(ORBIT_QUERIES))
+def test_orbit_fold(er2k, cl5k, loops_graph, monkeypatch, name):
+    """Symmetry breaking on the core of a query whose last vertex is a
+    pendant, weighted by the pendant's attachment orbit: counts against the
+    oracle through the fused kernel, the flattened kernel (no fusion), with
+    chunking, with every parent split into the fused kernel's second phase,
+    and against the plan that breaks the whole query's symmetry."""
+    k, arcs = ORBIT_QUERIES[name]
+    q = cb.Query.from_arcs(k, arcs)
+    lv, _ = q.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
+    assert lv[k - 1]["ofold"], name
+    S = cb.FLAG_SYMMETRY_BREAK
+    for h, g, od in (er2k, cl5k, loops_graph):
+        cnt, _, _ = oracle_count(od, k, arcs, q.order)
+        assert g.count(q, flags=S).count == cnt
+        assert g.count(q, flags=S | cb.FLAG_NO_FUSE).count == cnt
+        assert g.count(q, flags=S | cb.FLAG_NO_ORBIT_FOLD).count == cnt
+        assert g.count(q, flags=S, chunks=3).count == cnt
+        monkeypatch.setenv("CUTS_FUSE_SPLIT", "0")
+        assert g.count(q, flags=S).count == cnt
+        monkeypatch.delenv("CUTS_FUSE_SPLIT")

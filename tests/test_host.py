@@ -258,3 +258,109 @@ def test_converters(tmp_path):
     lines = (tmp_path / "q.gsi").read_text().splitlines()
     assert lines[0] == "t # 0" and lines[1] == "3 3 1 1" and lines[-1] == "t # -1"
     assert lines[2:5] == ["v 0 1", "v 1 1", "v 2 1"] and lines[5] == "e 0 1 1"
+
+
+def _und(edges):
+    return [(a, b) for u, v in edges for a, b in ((u, v), (v, u))]
+
+
+ORBIT_QUERIES = {
+    # name: (k, arcs, expected orbit size or 0 for "no orbit fold")
+    "4-clique+pendant": cb.named_query_arcs("4-clique+pendant") + (4,),
+    "paw": (4, _und([(0, 1), (1, 2), (0, 2), (0, 3)]), 3),
+    "5-clique+pendant": (6, _und([(a, b) for a in range(5) for b in range(a + 1, 5)] + [(0, 5)]), 5),
+    "4-cycle+pendant": (5, _und([(0, 1), (1, 2), (2, 3), (3, 0), (0, 4)]), 0),
+    "diamond+pendant-deg3": (5, _und([(0, 1), (0, 2), (1, 2), (1, 3), (2, 3), (1, 4)]), 0),
+    "diamond+pendant-deg2": (5, _und([(0, 1), (0, 2), (1, 2), (1, 3), (2, 3), (0, 4)]), 0),
+    "path4": (4, _und([(0, 1), (1, 2), (2, 3)]), 0),
+    "star4": (5, _und([(0, 1), (0, 2), (0, 3), (0, 4)]), 0),
+    # a directed 3-cycle with an out-pendant: the rotations move the attachment
+    "dir3cycle+pendant": (4, [(0, 1), (1, 2), (2, 0), (0, 3)], 3),
+}
+
+
+def _brute_orbit_total(q, qarcs, lv, aut, n, out_adj, in_adj):
+    """aut x sum over core embeddings that satisfy the plan's masks of the
+    orbit weight -- the orbit fold's formula evaluated by brute force."""
+    import itertools
+    k = q.k
+    order = q.order
+    e = order[k - 1]
+    arcs = set(qarcs)
+    core = order[:k - 1]
+    a = [v for v in core if (v, e) in arcs or (e, v) in arcs][0]
+    use_out = (a, e) in arcs
+    L = out_adj if use_out else in_adj
+    omask = lv[k - 1]["ofold"]
+    total = 0
+    for m in itertools.permutations(range(n), k - 1):
+        ok = True
+        for i in range(k - 1):
+            for j in range(k - 1):
+                if i != j and (core[i], core[j]) in arcs and m[j] not in out_adj[m[i]]:
+                    ok = False
+                    break
+                if j < i and ((lv[i]["gt"] >> j) & 1) and not m[i] > m[j]:
+                    ok = False
+                    break
+                if j < i and ((lv[i]["lt"] >> j) & 1) and not m[i] < m[j]:
+                    ok = False
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        mset = set(m)
+        for x in range(k - 1):
+            if (omask >> x) & 1:
+                total += len(L[m[x]] - mset)
+    return total * aut
+
+
+@pytest.mark.parametrize("name", sorted(ORBIT_QUERIES))
+@pytest.mark.parametrize("directed", [False, True])
+def test_orbit_fold_plan_is_exact(name, directed):
+    """The orbit fold's plan (core symmetry conditions, multiplier, orbit
+    positions) evaluated by brute force equals the oracle's count."""
+    k, arcs, _ = ORBIT_QUERIES[name]
+    rng = np.random.default_rng(7 + k)
+    n = 9
+    src, dst = [], []
+    for u in range(n):
+        for v in range(n):
+            if u != v and rng.random() < 0.55:
+                src.append(u); dst.append(v)
+                if not directed:
+                    src.append(v); dst.append(u)
+    if directed:
+        arcs = [(a, b) for a, b in arcs if a < b] + [(b, a) for a, b in arcs if a > b and (a + b) % 3 == 0]
+    out_adj = [set() for _ in range(n)]
+    in_adj = [set() for _ in range(n)]
+    for u, v in zip(src, dst):
+        out_adj[u].add(v)
+        in_adj[v].add(u)
+    sym = all(u in out_adj[v] for u in range(n) for v in out_adj[u])
+    q = cb.Query.from_arcs(k, arcs)
+    lv, aut = q.plan_levels(sym, cb.FLAG_SYMMETRY_BREAK)
+    og = O.Graph.from_arrays(n, np.array(src, np.uint32), np.array(dst, np.uint32))
+    want = O.count(og, O.Graph.from_arcs(k, arcs), q.order)[0]
+    if lv[k - 1]["ofold"]:
+        assert lv[k - 2]["fold"] == 1
+        got = _brute_orbit_total(q, arcs, lv, aut, n, out_adj, in_adj)
+        assert got == want, (name, directed, lv[k - 1]["ofold"], aut)
+    lvn, autn = q.plan_levels(sym, cb.FLAG_SYMMETRY_BREAK | cb.FLAG_NO_ORBIT_FOLD)
+    assert all(l["ofold"] == 0 for l in lvn)
+
+
+def test_orbit_fold_plan_shape():
+    q = cb.Query.from_arcs(*cb.named_query_arcs("4-clique+pendant"))
+    lv, aut = q.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
+    k = q.k
+    # core K4 (|Aut| 24), the pendant's clique vertex has an orbit of 4
+    assert bin(lv[k - 1]["ofold"]).count("1") == 4 and aut == 6
+    assert lv[k - 2]["fold"] == 1 and lv[k - 2]["fuse"] == 1
+    # the core's chain orders all four clique positions
+    assert lv[1]["gt"] and lv[2]["gt"] and lv[3]["gt"]
+    # without symmetry breaking: the plain fold, no orbit
+    lv0, aut0 = q.plan_levels(True, 0)
+    assert lv0[k - 1]["ofold"] == 0 and aut0 == 1
