@@ -304,14 +304,14 @@ class Query:
 
     def plan_levels(self, data_symmetric: bool = True, flags: int = 0):
         """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt, fuse,
-        ofold) and the count multiplier used."""
+        ofold, qin, qout) and the count multiplier used."""
         k = self.k
-        out = np.zeros(9 * k, np.uint32)
+        out = np.zeros(11 * k, np.uint32)
         aut = C.c_uint64()
         _check(lib().cuts_query_plan_levels(self._h, int(data_symmetric), flags, _ptr(out, _u32p),
                                             C.byref(aut)))
-        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse", "ofold"]
-        return [dict(zip(keys, (int(x) for x in out[9 * i:9 * i + 9]))) for i in range(k)], aut.value
+        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse", "ofold", "qin", "qout"]
+        return [dict(zip(keys, (int(x) for x in out[11 * i:11 * i + 11]))) for i in range(k)], aut.value
 
     def automorphisms(self) -> int:
         a = C.c_uint64()

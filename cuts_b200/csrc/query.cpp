@@ -314,6 +314,13 @@ static bool orbit_fold_plan(const Query &q, bool data_symmetric, Plan &plan) {
         else plan.lv[pa].lt_mask |= 1u << pb;
     }
     plan.aut = autc / uint64_t(__builtin_popcount(omask));
+    // the core's positions are filtered by their degrees in the core: an
+    // orbit vertex other than a carries no pendant arc, and the class
+    // representative may put any orbit vertex at a's position
+    for (uint32_t i = 0; i + 1 < k; ++i) {
+        plan.lv[i].qin = uint32_t(C.in[i].size());
+        plan.lv[i].qout = uint32_t(C.out[i].size());
+    }
     F.ofold = omask;
     for (uint32_t x = 0; x < kMaxK; ++x) F.oguar[x] = oguar[x];
     plan.lv[k - 2].fold = 1;

@@ -144,10 +144,11 @@ int cuts_query_joins(cuts_query q, uint32_t *p_off, uint32_t *p, uint32_t *c_off
 int cuts_query_set_order(cuts_query q, const uint32_t *order);
 
 /* The per-level plan the kernels run for the current order, for a data
- * graph that is symmetric or not and the given flags: 9 words per level,
+ * graph that is symmetric or not and the given flags: 11 words per level,
  * {joined lists, signature test, closed form, folded into the level before,
  * guaranteed-member mask, greater-than mask, less-than mask, fused with the
- * level before, orbit-fold positions}.  Host only;
+ * level before, orbit-fold positions, signature in-degree, signature
+ * out-degree}.  Host only;
  * no reference counterpart (the reference derives joins per launch,
  * device_funcs.cu:103-127). */
 int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,

@@ -382,7 +382,17 @@ def test_orbit_fold(er2k, cl5k, loops_graph, monkeypatch, name):
     lv, _ = q.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
     assert lv[k - 1]["ofold"], name
     S = cb.FLAG_SYMMETRY_BREAK
-    for h, g, od in (er2k, cl5k, loops_graph):
+    # a graph whose lowest clique vertices have no other edges: a class
+    # representative puts a vertex without a pendant neighbour first
+    und = ([(a, b) for a in range(5) for b in range(a + 1, 5)] + [(4, 5), (4, 6), (1, 5), (2, 5)] +
+           [(9, 10), (9, 11), (10, 11), (10, 12), (10, 13)] +
+           [(a, b) for a in range(14, 18) for b in range(a + 1, 18)] + [(17, 18), (17, 19)] +
+           [(a, b) for a in range(20, 26) for b in range(a + 1, 26)] + [(25, 26)])
+    src = np.array([a for a, b in und] + [b for a, b in und], np.uint32)
+    dst = np.array([b for a, b in und] + [a for a, b in und], np.uint32)
+    oo, oa, io, ia, s_, d_ = csr_from_arcs(27, src, dst)
+    edge = (None, cb.Graph.from_csr(27, oo, oa, io, ia), O.Graph.from_arrays(27, s_, d_))
+    for h, g, od in (er2k, cl5k, loops_graph, edge):
         cnt, _, _ = oracle_count(od, k, arcs, q.order)
         assert g.count(q, flags=S).count == cnt
         assert g.count(q, flags=S | cb.FLAG_NO_FUSE).count == cnt

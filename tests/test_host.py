@@ -280,58 +280,97 @@ ORBIT_QUERIES = {
 
 
 def _brute_orbit_total(q, qarcs, lv, aut, n, out_adj, in_adj):
-    """aut x sum over core embeddings that satisfy the plan's masks of the
-    orbit weight -- the orbit fold's formula evaluated by brute force."""
-    import itertools
+    """aut x sum over core embeddings that satisfy the plan's masks and
+    signatures of the orbit weight -- the orbit fold's formula evaluated by
+    a plain depth-first search."""
     k = q.k
     order = q.order
     e = order[k - 1]
     arcs = set(qarcs)
     core = order[:k - 1]
     a = [v for v in core if (v, e) in arcs or (e, v) in arcs][0]
-    use_out = (a, e) in arcs
-    L = out_adj if use_out else in_adj
+    L = out_adj if (a, e) in arcs else in_adj
     omask = lv[k - 1]["ofold"]
     total = 0
-    for m in itertools.permutations(range(n), k - 1):
-        ok = True
-        for i in range(k - 1):
-            for j in range(k - 1):
-                if i != j and (core[i], core[j]) in arcs and m[j] not in out_adj[m[i]]:
-                    ok = False
-                    break
-                if j < i and ((lv[i]["gt"] >> j) & 1) and not m[i] > m[j]:
-                    ok = False
-                    break
-                if j < i and ((lv[i]["lt"] >> j) & 1) and not m[i] < m[j]:
-                    ok = False
-                    break
-            if not ok:
-                break
-        if not ok:
-            continue
-        mset = set(m)
-        for x in range(k - 1):
-            if (omask >> x) & 1:
-                total += len(L[m[x]] - mset)
+    m = []
+
+    def fits(i, v):
+        if v in m:
+            return False
+        if lv[i]["sig"] and (len(in_adj[v]) < lv[i]["qin"] or len(out_adj[v]) < lv[i]["qout"]):
+            return False
+        for j in range(i):
+            if (core[i], core[j]) in arcs and m[j] not in out_adj[v]:
+                return False
+            if (core[j], core[i]) in arcs and v not in out_adj[m[j]]:
+                return False
+            if ((lv[i]["gt"] >> j) & 1) and not v > m[j]:
+                return False
+            if ((lv[i]["lt"] >> j) & 1) and not v < m[j]:
+                return False
+        return True
+
+    def dfs(i):
+        nonlocal total
+        if i == k - 1:
+            mset = set(m)
+            for x in range(k - 1):
+                if (omask >> x) & 1:
+                    total += len(L[m[x]] - mset)
+            return
+        for v in range(n):
+            if fits(i, v):
+                m.append(v)
+                dfs(i + 1)
+                m.pop()
+
+    dfs(0)
     return total * aut
+
+
+def _orbit_graphs(directed, k):
+    """Small data graphs: random ones, dense and sparse, and one whose
+    lowest-id clique vertices have no edges outside their clique (so a class
+    representative puts a vertex without a pendant neighbour at the
+    attachment's position)."""
+    out = []
+    for dens in (0.55, 0.3):
+        rng = np.random.default_rng(7 + k)
+        n = 9
+        src, dst = [], []
+        for u in range(n):
+            for v in range(n):
+                if u != v and rng.random() < dens:
+                    src.append(u); dst.append(v)
+                    if not directed:
+                        src.append(v); dst.append(u)
+        out.append((n, src, dst))
+    # K5 on 0..4 with pendants on 4; a triangle 9-10-11 whose lowest vertex
+    # has no other edge; a K4 14..17 whose lowest three have no other edge;
+    # a K6 20..25 with one extra edge on 25
+    und = ([(a, b) for a in range(5) for b in range(a + 1, 5)] + [(4, 5), (4, 6), (4, 7), (4, 8),
+                                                                   (1, 5), (2, 5), (2, 6)] +
+           [(9, 10), (9, 11), (10, 11), (10, 12), (10, 13)] +
+           [(a, b) for a in range(14, 18) for b in range(a + 1, 18)] + [(17, 18), (17, 19)] +
+           [(a, b) for a in range(20, 26) for b in range(a + 1, 26)] + [(25, 26)])
+    src = [a for a, b in und] + ([] if directed else [b for a, b in und])
+    dst = [b for a, b in und] + ([] if directed else [a for a, b in und])
+    out.append((27, src, dst))
+    return out
 
 
 @pytest.mark.parametrize("name", sorted(ORBIT_QUERIES))
 @pytest.mark.parametrize("directed", [False, True])
 def test_orbit_fold_plan_is_exact(name, directed):
-    """The orbit fold's plan (core symmetry conditions, multiplier, orbit
-    positions) evaluated by brute force equals the oracle's count."""
+    """The orbit fold's plan (core symmetry conditions, signatures,
+    multiplier, orbit positions) evaluated by brute force equals the
+    oracle's count."""
     k, arcs, _ = ORBIT_QUERIES[name]
-    rng = np.random.default_rng(7 + k)
-    n = 9
-    src, dst = [], []
-    for u in range(n):
-        for v in range(n):
-            if u != v and rng.random() < 0.55:
-                src.append(u); dst.append(v)
-                if not directed:
-                    src.append(v); dst.append(u)
+    for n, src, dst in _orbit_graphs(directed, k):
+        _orbit_case(name, directed, k, arcs, n, src, dst)
+
+
+def _orbit_case(name, directed, k, arcs, n, src, dst):
     if directed:
         arcs = [(a, b) for a, b in arcs if a < b] + [(b, a) for a, b in arcs if a > b and (a + b) % 3 == 0]
     out_adj = [set() for _ in range(n)]
