@@ -100,6 +100,8 @@ _SIGS = {
     "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "cuts_batch_info": (C.c_int, [_vp, _u64p, _u32p]),
     "cuts_batch_set_query_budget": (C.c_int, [_vp, C.c_double]),
+    "cuts_plan_candidates": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint32, _u32p,
+                                       C.POINTER(C.c_double), _u32p]),
     "cuts_batch_free": (None, [_vp]),
     "cuts_count_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.POINTER(_vp), C.c_uint32,
                                      C.c_uint32, _vp, _vp]),
@@ -301,6 +303,17 @@ class Query:
         _check(lib().cuts_plan(self._h, graph._h, mode, model._h if model else None, beam, margin,
                                _ptr(o, _u32p), C.byref(pw), C.byref(sw)))
         return [int(x) for x in o], pw.value, sw.value
+
+    def candidates(self, graph: "Graph", model: "Mlp", count: int = 4, beam: int = 256):
+        """The `count` orders with the least predicted work under `model`
+        (least first) as [(order, predicted work)]; the query's order is kept."""
+        k = self.k
+        o = np.zeros(max(count, 1) * k, np.uint32)
+        w = (C.c_double * max(count, 1))()
+        n = C.c_uint32()
+        _check(lib().cuts_plan_candidates(self._h, graph._h, model._h, beam, count, _ptr(o, _u32p), w,
+                                          C.byref(n)))
+        return [([int(x) for x in o[r * k:(r + 1) * k]], w[r]) for r in range(n.value)]
 
     def plan_levels(self, data_symmetric: bool = True, flags: int = 0):
         """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt, fuse,

@@ -528,6 +528,26 @@ int cuts_plan(cuts_query q, cuts_graph g, int mode, cuts_mlp m, uint32_t beam, d
     })());
 }
 
+int cuts_plan_candidates(cuts_query q, cuts_graph g, cuts_mlp m, uint32_t beam, uint32_t max_orders,
+                         uint32_t *orders_out, double *work_out, uint32_t *n_out) {
+    if (!q || !g || !g->dev || !m || !orders_out || !n_out) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(([&]() {
+        const Query &Q = q->q;
+        OrderSearchOptions opt;
+        opt.beam = beam;
+        opt.top = max_orders;
+        OrderChoice ch;
+        int rc = learned_order(Q, g->dev->stats, m->m, opt, ch);
+        if (rc) return rc;
+        *n_out = uint32_t(ch.top.size());
+        for (size_t r = 0; r < ch.top.size(); ++r) {
+            std::copy(ch.top[r].begin(), ch.top[r].end(), orders_out + r * Q.k);
+            if (work_out) work_out[r] = ch.top_work[r];
+        }
+        return CUTS_OK;
+    })());
+}
+
 int cuts_batch_create(cuts_graph g, const cuts_query *qs, uint32_t nq, uint32_t flags,
                       const uint32_t *tune, cuts_batch *out) {
     if (!g || !g->dev || !out || (nq && !qs)) return set_error(CUTS_ERR_ARG, "null argument");

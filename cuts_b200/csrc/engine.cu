@@ -702,8 +702,10 @@ struct FusedBig {
     unsigned long long pool_words;
 };
 
+// 12 resident blocks (48 warps) per SM: the kernel waits on dependent L2
+// loads, and the extra warps outweigh the spills the 40-register cap costs
 template <int MODE>
-__global__ void __launch_bounds__(kZW * 32)
+__global__ void __launch_bounds__(kZW * 32, 12)
 k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb, uint32_t phase,
         uint32_t split, uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride, FusedBig big,
         unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,

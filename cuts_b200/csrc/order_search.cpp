@@ -209,6 +209,17 @@ int learned_order(const Query &q, const DegreeStats &ds, Mlp &mlp, const OrderSe
         if (w < bw) { bw = w; best = r; }
     }
     out.best_work = bw;
+    if (opt.top) {
+        std::vector<std::pair<double, size_t>> key;
+        for (size_t r = 0; r < cur.size(); ++r)
+            if (cur[r].order.size() == k)
+                key.push_back({predicted_work(q, cur[r].order.data(), cur[r].pred.data()), r});
+        std::sort(key.begin(), key.end());
+        for (size_t r = 0; r < key.size() && r < opt.top; ++r) {
+            out.top.push_back(cur[key[r].second].order);
+            out.top_work.push_back(key[r].first);
+        }
+    }
     if (!cur.empty() && bw * opt.margin < out.score_work) {
         out.order = cur[best].order;
         out.pred = cur[best].pred;

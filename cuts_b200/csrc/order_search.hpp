@@ -33,6 +33,7 @@ double predicted_work(const Query &q, const uint32_t *order, const float *pred);
 struct OrderSearchOptions {
     size_t beam = 0;      // 0 = exhaustive
     double margin = 1.25; // learned order must promise this much less work
+    size_t top = 0;       // also return this many complete orders, least predicted work first
 };
 
 struct OrderChoice {
@@ -41,6 +42,8 @@ struct OrderChoice {
     double best_work = 0, score_work = 0;
     size_t candidates = 0;
     bool used_learned = false;
+    std::vector<std::vector<uint32_t>> top;  // opt.top best complete orders
+    std::vector<double> top_work;
 };
 
 int learned_order(const Query &q, const DegreeStats &ds, Mlp &mlp, const OrderSearchOptions &opt,

@@ -129,3 +129,24 @@ def work(levels: Sequence[int], k: int, joins: Sequence[int]) -> float:
 def joins_of(q: "cb.Query") -> List[int]:
     P, C = q.joins()
     return [len(set(P[i]) | set(C[i])) for i in range(q.k)]
+
+
+def choose_order(g: "cb.Graph", q: "cb.Query", model: "cb.Mlp", proposals: int = 3, beam: int = 256,
+                 stride: int = 1 << 16, budget_ms: float = 50.0, flags: int = 0):
+    """Learned proposals, measured choice: the model's `proposals` best orders
+    and the score order are each timed on the same root stripe
+    (u % stride == 0, under budget_ms); the fastest is set on q.  The score
+    order wins ties and stays when no proposal finishes its stripe faster.
+    Returns (order, {order tuple: stripe ms or None})."""
+    score = list(q.order)
+    cands = [score] + [o for o, _ in q.candidates(g, model, proposals, beam) if o != score]
+    times = {}
+    best, best_ms = score, None
+    for o in cands:
+        q.set_order(o)
+        r, done = g.count_sample(q, 0, stride, budget_ms, flags)
+        times[tuple(o)] = r.ms if done else None
+        if done and (best_ms is None or r.ms < best_ms * (0.9 if o != score else 1.0)):
+            best, best_ms = o, r.ms
+    q.set_order(best)
+    return best, times

@@ -80,9 +80,9 @@ def plain_pass(g: "cb.Graph", queries, budget_ms: float, flags: int = 0, orders=
     return res, time.perf_counter() - t0
 
 
-def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1 << 14,
+def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, stride: int = 1 << 16,
                 epochs: int = 400, seed: int = 10000, time_budget_s: float = 120.0,
-                run_budget_ms: float = 200.0):
+                run_budget_ms: float = 100.0):
     train_q = eval_queries(n_train, seed0=seed)
     t0 = time.perf_counter()
     samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
@@ -101,10 +101,10 @@ def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, s
 
 
 def estimate_orders(g: "cb.Graph", qdefs, orders_a, orders_b, stride: int, budget_ms: float,
-                    flags: int = 0):
+                    flags: int = 0, shard: int = 1):
     """Estimated device time of a full exact count of each query under two
-    orders, from the same root stripe (u % stride == 0; the stripe's time x
-    stride); None where the stripe itself exceeds budget_ms."""
+    orders, from the same root stripe (u % stride == shard; the stripe's time
+    x stride); None where the stripe itself exceeds budget_ms."""
     out = []
     t0 = time.perf_counter()
     for i, (k, arcs) in enumerate(qdefs):
@@ -112,7 +112,7 @@ def estimate_orders(g: "cb.Graph", qdefs, orders_a, orders_b, stride: int, budge
         for orders in (orders_a, orders_b):
             q = cb.Query.from_arcs(k, arcs)
             q.set_order(orders[i])
-            r, done = g.count_sample(q, 0, stride, budget_ms, flags)
+            r, done = g.count_sample(q, shard, stride, budget_ms, flags)
             row.append(r.ms * stride if done else None)
         out.append(row)
         if (i + 1) % 50 == 0:
@@ -120,17 +120,22 @@ def estimate_orders(g: "cb.Graph", qdefs, orders_a, orders_b, stride: int, budge
     return out
 
 
-def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 250.0,
+def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 100.0,
                 model=None, train_budget_s: float = 120.0, flags: int = 0,
                 est_stride: int = 1 << 12, est_budget_ms: float = 300.0):
     """The 200 evaluation queries three ways, each query under the same
     budget of budget_ms of the whole GPU:
       plain    -- score order, level engine, one query at a time;
-      learned  -- the learned order, level engine, one query at a time;
+      learned  -- the learned order (the model's three best proposals and the
+                  score order timed on a small root stripe, the fastest
+                  kept), level engine, one query at a time;
       learned_batched -- the learned order, all queries in one persistent
-                  launch (cheapest predicted first), each limited to
+                  launch (cheapest measured first), each limited to
                   budget_ms of GPU time by the batched kernel's per-query limit.
-    queries/s = finished queries / seconds (planning included)."""
+    queries/s = finished queries / seconds (planning included).  Alongside:
+    the estimated device time of each query's full exact count under the
+    score and the learned order, from another root stripe (shard 1), so the
+    choice and its evaluation use different roots."""
     info = {}
     if model is None:
         model, info = train_model(g, n_train=n_train, time_budget_s=train_budget_s)
@@ -138,16 +143,23 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
     plain, plain_s = plain_pass(g, qdefs, budget_ms, flags)
     t0 = time.perf_counter()
     qs, works, orders = [], [], []
-    switched = 0
+    switched = model_switched = 0
     for k, arcs in qdefs:
         q = cb.Query.from_arcs(k, arcs)
-        order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, beam=256)
-        switched += pw < sw
+        score = list(q.order)
+        _, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, beam=256, margin=2.0)
+        model_switched += pw < sw
+        q.set_order(score)
+        # the model's proposals, measured on a small root stripe (shard 0)
+        order, times = L.choose_order(g, q, model, proposals=3, flags=flags)
+        switched += order != score
         qs.append(q)
-        works.append(pw)
+        t = times.get(tuple(order))
+        works.append(t if t is not None else math.inf)
         orders.append(order)
     plan_s = time.perf_counter() - t0
-    _log(f"planned {n_eval} queries in {plan_s:.1f} s, {switched} orders changed")
+    _log(f"planned {n_eval} queries in {plan_s:.1f} s: {switched} orders changed by measured "
+         f"proposals, {model_switched} by the model alone")
     score_orders = [cb.Query.from_arcs(k, arcs).order for k, arcs in qdefs]
     est = estimate_orders(g, qdefs, score_orders, orders, est_stride, est_budget_ms, flags)
     both = [(a, b) for a, b in est if a is not None and b is not None]
@@ -167,7 +179,7 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
     }
     _log(f"estimates: {est_rep}")
     learned, learned_s = plain_pass(g, qdefs, budget_ms, flags, orders=orders, tag="learned")
-    # cheapest predicted work first
+    # cheapest measured stripe first
     rank = sorted(range(n_eval), key=lambda i: works[i])
     b = g.batch([qs[i] for i in rank], flags=flags)
     b.set_query_budget(budget_ms)
@@ -191,6 +203,7 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
                   "queries_per_s": sum(done_p) / plain_s, "finished_by_k": fin_k(done_p)},
         "learned": {"finished": sum(done_l), "seconds": plan_s + learned_s, "plan_s": plan_s,
                     "queries_per_s": sum(done_l) / (plan_s + learned_s), "orders_changed": switched,
+                    "orders_changed_by_model_alone": model_switched,
                     "finished_by_k": fin_k(done_l)},
         "learned_batched": {"finished": sum(done_b), "seconds": lb_s, "plan_s": plan_s,
                             "launch_ms": ms, "launch_wall_s": batch_wall,

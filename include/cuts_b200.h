@@ -255,6 +255,14 @@ int cuts_query_features(cuts_query q, cuts_graph g, const uint32_t *order,
 int cuts_plan(cuts_query q, cuts_graph g, int mode, cuts_mlp m, uint32_t beam, double margin,
               uint32_t *order_out, double *pred_work, double *score_work);
 
+/* The max_orders complete orders with the least predicted work under the
+ * model m (same search as cuts_plan), least first, without changing the
+ * query's order: orders_out holds max_orders x k entries, work_out (may be
+ * NULL) max_orders values; *n_out receives how many were found.  Lets a
+ * caller measure a few proposals on a root stripe and keep the fastest. */
+int cuts_plan_candidates(cuts_query q, cuts_graph g, cuts_mlp m, uint32_t beam, uint32_t max_orders,
+                         uint32_t *orders_out, double *work_out, uint32_t *n_out);
+
 /* ---- batched counting -------------------------------------------- */
 
 /* Count nq queries against one resident graph in one persistent launch.

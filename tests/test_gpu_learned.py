@@ -76,3 +76,29 @@ def test_score_order_judges_predictions(setup):
         samples.append(L.Sample(i, q.order, lv, ms, True))
     X, y, _ = L.features(g, eval_q, samples)
     assert L.prediction_error(model, X, y) < 1.5
+
+
+def test_candidates_and_measured_choice(setup):
+    """The model's best orders come least predicted work first, are valid
+    connected orders, and the measured choice among them and the score order
+    keeps the count and is never slower on its own stripe than the score
+    order by more than the tie margin."""
+    g, model, _, eval_q, _ = setup
+    for k, arcs in eval_q[:10]:
+        q = cb.Query.from_arcs(k, arcs)
+        score = list(q.order)
+        c = q.candidates(g, model, count=4, beam=64)
+        assert 1 <= len(c) <= 4
+        works = [w for _, w in c]
+        assert works == sorted(works)
+        for o, _ in c:
+            assert sorted(o) == list(range(k))
+            q.set_order(o)  # rejects an order with an unjoined prefix
+        assert q.order == c[-1][0]
+        q.set_order(score)
+        want = g.count(q).count
+        order, times = L.choose_order(g, q, model, proposals=3, stride=16, budget_ms=1000.0)
+        assert q.order == order
+        assert g.count(q).count == want
+        if times[tuple(score)] is not None and tuple(order) != tuple(score):
+            assert times[tuple(order)] < times[tuple(score)]
