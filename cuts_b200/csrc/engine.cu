@@ -1336,14 +1336,41 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     *out = nullptr;
     CK(cudaSetDevice(device));
     const uint32_t n = hg.n;
+    // Device vertex ids are degree ranks: orig[d] is the host vertex stored
+    // as d, in order of (out + in degree, id), so hubs get the highest ids.
+    // Counts do not depend on the labelling; with symmetry breaking, the
+    // class representative (m_a < m_b conditions) then starts from its
+    // lowest-degree vertex and candidate windows "above" a vertex hold only
+    // vertices of higher degree, which bounds them on power-law graphs.
+    // CUTS_NO_RELABEL=1 keeps the host ids (comparisons).
+    const char *nr = std::getenv("CUTS_NO_RELABEL");
+    const bool relabel = !(nr && nr[0] == '1') && n > 1;
+    std::vector<uint32_t> orig, rank;
+    if (relabel) {
+        // stable counting sort by degree
+        const uint32_t maxd = 2 * hg.max_degree() + 1;
+        std::vector<uint64_t> cnt(size_t(maxd) + 2, 0);
+        auto deg = [&](uint32_t v) { return hg.out_deg(v) + (hg.symmetric ? 0 : hg.in_deg(v)); };
+        for (uint32_t v = 0; v < n; ++v) cnt[deg(v) + 1]++;
+        for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
+        orig.resize(n);
+        rank.resize(n);
+        for (uint32_t v = 0; v < n; ++v) {
+            const uint32_t d = uint32_t(cnt[deg(v)]++);
+            orig[d] = v;
+            rank[v] = d;
+        }
+    }
+    auto host_of = [&](uint32_t d) { return relabel ? orig[d] : d; };
     // padded layout: every list starts at a multiple of 4 words
     auto build = [&](bool in_dir, std::vector<uint2> &info, uint64_t &words) {
         info.resize(n);
         uint64_t w = 0;
-        for (uint32_t v = 0; v < n; ++v) {
-            const uint32_t d = in_dir ? hg.in_deg(v) : hg.out_deg(v);
-            info[v] = make_uint2(uint32_t(w), d);
-            w += (uint64_t(d) + 3) & ~uint64_t(3);
+        for (uint32_t d = 0; d < n; ++d) {
+            const uint32_t v = host_of(d);
+            const uint32_t len = in_dir ? hg.in_deg(v) : hg.out_deg(v);
+            info[d] = make_uint2(uint32_t(w), len);
+            w += (uint64_t(len) + 3) & ~uint64_t(3);
         }
         words = w;
     };
@@ -1358,10 +1385,19 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
         for (auto &x : iinfo) x.x += uint32_t(owords);
     std::vector<uint32_t> adj(std::max<uint64_t>(total_words, 4), 0xffffffffu);
     #pragma omp parallel for schedule(dynamic, 4096)
-    for (int64_t v = 0; v < int64_t(n); ++v) {
-        std::memcpy(adj.data() + oinfo[v].x, hg.out_list(uint32_t(v)), sizeof(uint32_t) * oinfo[v].y);
-        if (!hg.symmetric)
-            std::memcpy(adj.data() + iinfo[v].x, hg.in_list(uint32_t(v)), sizeof(uint32_t) * iinfo[v].y);
+    for (int64_t d = 0; d < int64_t(n); ++d) {
+        const uint32_t v = host_of(uint32_t(d));
+        auto put = [&](const uint32_t *src, uint2 inf) {
+            uint32_t *dst = adj.data() + inf.x;
+            if (!relabel) {
+                std::memcpy(dst, src, sizeof(uint32_t) * inf.y);
+                return;
+            }
+            for (uint32_t i = 0; i < inf.y; ++i) dst[i] = rank[src[i]];
+            std::sort(dst, dst + inf.y);
+        };
+        put(hg.out_list(v), oinfo[d]);
+        if (!hg.symmetric) put(hg.in_list(v), iinfo[d]);
     }
     auto *g = new DeviceGraph();
     g->device = device;
@@ -1382,10 +1418,11 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     g->stats = degree_stats(hg);
     g->h_out_deg.resize(n);
     g->h_in_deg.resize(n);
-    for (uint32_t v = 0; v < n; ++v) {
-        g->h_out_deg[v] = hg.out_deg(v);
-        g->h_in_deg[v] = hg.in_deg(v);
+    for (uint32_t d = 0; d < n; ++d) {
+        g->h_out_deg[d] = hg.out_deg(host_of(d));
+        g->h_in_deg[d] = hg.in_deg(host_of(d));
     }
+    g->orig.swap(orig);
     auto fail = [&](cudaError_t e, const char *what) {
         device_graph_free(g);
         return set_error(CUTS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -1872,7 +1909,7 @@ int Run::write_rows(uint32_t nout) {
                 *w++ = '(';
                 w = std::to_chars(w, end, order[j]).ptr;
                 *w++ = ',';
-                w = std::to_chars(w, end, row[j]).ptr;
+                w = std::to_chars(w, end, g.orig.empty() ? row[j] : g.orig[row[j]]).ptr;
                 *w++ = ')';
             }
             *w++ = '\n';

@@ -43,7 +43,8 @@ struct DeviceGraph {
     uint32_t *h_bounds = nullptr;          // pinned
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DegreeStats stats;                     // degree tails, for order features
-    std::vector<uint32_t> h_out_deg, h_in_deg;
+    std::vector<uint32_t> h_out_deg, h_in_deg;  // by device id
+    std::vector<uint32_t> orig;            // device id -> host vertex (empty: the same)
 
     // batched engine: vertices in out-degree order and task prefix sums
     uint32_t *batch_vsorted = nullptr;
