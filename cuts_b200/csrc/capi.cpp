@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <memory>
@@ -182,11 +183,8 @@ int cuts_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out
     if (!out) return set_error(CUTS_ERR_ARG, "null argument");
     *out = nullptr;
     GUARD(([&]() {
-        HostGraph g;
-        int rc = graph_from_csr(n, out_off, out_adj, in_off, in_adj, g);
-        if (rc) return rc;
         auto gh = std::make_unique<cuts_graph_s>();
-        rc = device_graph_upload(g, device, &gh->dev);
+        int rc = device_graph_from_csr(n, out_off, out_adj, in_off, in_adj, device, &gh->dev);
         if (rc) return rc;
         *out = gh.release();
         return CUTS_OK;
@@ -416,6 +414,11 @@ int cuts_search(const char *query_file, const char *data_file, int write_to_disk
         CountResult r;
         CountOptions opt;
         opt.chunks = trunks ? trunks : 1;
+        // the same count, found once per automorphism class (exact; a query
+        // with self-loops is enumerated plainly); CUTS_PLAIN=1 enumerates
+        // every embedding as the reference does
+        const char *plain = std::getenv("CUTS_PLAIN");
+        if (!(plain && plain[0] == '1')) opt.flags = CUTS_FLAG_SYMMETRY_BREAK;
         rc = device_count(*dg, q, opt, r);
         if (rc) return rc;
         std::cout << base_name(data_file) << "," << base_name(query_file) << "," << r.ms << "ms,"

@@ -853,8 +853,8 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 const uint32_t o_oend = __shfl_sync(kFullMask, oend, ow);
                 const uint32_t o_iters = __shfl_sync(kFullMask, iters, ow);
                 uint32_t o_fbase = 0, o_foff = 0, o_fdeg = 0, o_flo = 0, o_fhi = 0;
-                if (cfold) {
-                    o_fbase = __shfl_sync(kFullMask, fbase, ow);
+                if (cfold) o_fbase = __shfl_sync(kFullMask, fbase, ow);
+                if (cfold && !sF.ofold) {  // the plain fold's list and window
                     o_foff = __shfl_sync(kFullMask, foff, ow);
                     o_fdeg = __shfl_sync(kFullMask, fdeg, ow);
                     o_flo = __shfl_sync(kFullMask, flo, ow);
@@ -1332,119 +1332,26 @@ constexpr int kU64Stamp = 5;  // d_u64 slot: device clock at the start of a budg
 
 // ---- upload -------------------------------------------------------------
 
-int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
+// Allocates a DeviceGraph, builds its layout on the device from CSR arrays
+// in host memory (layout.cu) and the engine's scratch.
+static int device_graph_build(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj,
+                              const uint64_t *in_off, const uint32_t *in_adj, int sym_hint, bool validate,
+                              int device, DeviceGraph **out) {
     *out = nullptr;
     CK(cudaSetDevice(device));
-    const uint32_t n = hg.n;
-    // Device vertex ids are degree ranks: orig[d] is the host vertex stored
-    // as d, in order of (out + in degree, id), so hubs get the highest ids.
-    // Counts do not depend on the labelling; with symmetry breaking, the
-    // class representative (m_a < m_b conditions) then starts from its
-    // lowest-degree vertex and candidate windows "above" a vertex hold only
-    // vertices of higher degree, which bounds them on power-law graphs.
-    // CUTS_NO_RELABEL=1 keeps the host ids (comparisons).
-    const char *nr = std::getenv("CUTS_NO_RELABEL");
-    const bool relabel = !(nr && nr[0] == '1') && n > 1;
-    std::vector<uint32_t> orig, rank;
-    if (relabel) {
-        // stable counting sort by degree
-        const uint32_t maxd = 2 * hg.max_degree() + 1;
-        std::vector<uint64_t> cnt(size_t(maxd) + 2, 0);
-        auto deg = [&](uint32_t v) { return hg.out_deg(v) + (hg.symmetric ? 0 : hg.in_deg(v)); };
-        for (uint32_t v = 0; v < n; ++v) cnt[deg(v) + 1]++;
-        for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
-        orig.resize(n);
-        rank.resize(n);
-        for (uint32_t v = 0; v < n; ++v) {
-            const uint32_t d = uint32_t(cnt[deg(v)]++);
-            orig[d] = v;
-            rank[v] = d;
-        }
-    }
-    auto host_of = [&](uint32_t d) { return relabel ? orig[d] : d; };
-    // padded layout: every list starts at a multiple of 4 words
-    auto build = [&](bool in_dir, std::vector<uint2> &info, uint64_t &words) {
-        info.resize(n);
-        uint64_t w = 0;
-        for (uint32_t d = 0; d < n; ++d) {
-            const uint32_t v = host_of(d);
-            const uint32_t len = in_dir ? hg.in_deg(v) : hg.out_deg(v);
-            info[d] = make_uint2(uint32_t(w), len);
-            w += (uint64_t(len) + 3) & ~uint64_t(3);
-        }
-        words = w;
-    };
-    std::vector<uint2> oinfo, iinfo;
-    uint64_t owords = 0, iwords = 0;
-    build(false, oinfo, owords);
-    if (!hg.symmetric) build(true, iinfo, iwords);
-    const uint64_t total_words = owords + iwords;
-    if (total_words >= (uint64_t(1) << 32))
-        return set_error(CUTS_ERR_LIMIT, "padded adjacency exceeds 2^32 words");
-    if (!hg.symmetric)
-        for (auto &x : iinfo) x.x += uint32_t(owords);
-    std::vector<uint32_t> adj(std::max<uint64_t>(total_words, 4), 0xffffffffu);
-    #pragma omp parallel for schedule(dynamic, 4096)
-    for (int64_t d = 0; d < int64_t(n); ++d) {
-        const uint32_t v = host_of(uint32_t(d));
-        auto put = [&](const uint32_t *src, uint2 inf) {
-            uint32_t *dst = adj.data() + inf.x;
-            if (!relabel) {
-                std::memcpy(dst, src, sizeof(uint32_t) * inf.y);
-                return;
-            }
-            for (uint32_t i = 0; i < inf.y; ++i) dst[i] = rank[src[i]];
-            std::sort(dst, dst + inf.y);
-        };
-        put(hg.out_list(v), oinfo[d]);
-        if (!hg.symmetric) put(hg.in_list(v), iinfo[d]);
-    }
     auto *g = new DeviceGraph();
     g->device = device;
-    g->n = n;
-    g->arcs = hg.arcs;
-    g->symmetric = hg.symmetric;
-    g->max_deg = hg.max_degree();
-    {
-        bool loops = false;
-        #pragma omp parallel for reduction(|| : loops) schedule(static)
-        for (int64_t v = 0; v < int64_t(n); ++v) {
-            const uint32_t *l = hg.out_list(uint32_t(v));
-            if (std::binary_search(l, l + hg.out_deg(uint32_t(v)), uint32_t(v))) loops = true;
-        }
-        g->loops = loops;
-    }
-    g->adj_words = adj.size();
-    g->stats = degree_stats(hg);
-    g->h_out_deg.resize(n);
-    g->h_in_deg.resize(n);
-    for (uint32_t d = 0; d < n; ++d) {
-        g->h_out_deg[d] = hg.out_deg(host_of(d));
-        g->h_in_deg[d] = hg.in_deg(host_of(d));
-    }
-    g->orig.swap(orig);
     auto fail = [&](cudaError_t e, const char *what) {
         device_graph_free(g);
         return set_error(CUTS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking))) return fail(e, "stream");
-    if ((e = cudaMalloc(&g->out_info, sizeof(uint2) * std::max<uint32_t>(n, 1)))) return fail(e, "cudaMalloc info");
-    if (!hg.symmetric) {
-        if ((e = cudaMalloc(&g->in_info, sizeof(uint2) * std::max<uint32_t>(n, 1)))) return fail(e, "cudaMalloc info");
-    } else {
-        g->in_info = g->out_info;
+    int rc = device_layout(n, out_off, out_adj, in_off, in_adj, sym_hint, validate, *g);
+    if (rc) {
+        device_graph_free(g);
+        return rc;
     }
-    if ((e = cudaMalloc(&g->adj, sizeof(uint32_t) * adj.size()))) return fail(e, "cudaMalloc adjacency");
-    if (n) {
-        if ((e = cudaMemcpyAsync(g->out_info, oinfo.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, g->stream)))
-            return fail(e, "upload");
-        if (!hg.symmetric &&
-            (e = cudaMemcpyAsync(g->in_info, iinfo.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, g->stream)))
-            return fail(e, "upload");
-    }
-    if ((e = cudaMemcpyAsync(g->adj, adj.data(), sizeof(uint32_t) * adj.size(), cudaMemcpyHostToDevice, g->stream)))
-        return fail(e, "upload");
     if ((e = cudaMalloc(&g->d_u32, sizeof(uint32_t) * kSlots))) return fail(e, "scratch");
     if ((e = cudaMalloc(&g->d_u64, sizeof(unsigned long long) * 8))) return fail(e, "scratch");
     if ((e = cudaMalloc(&g->d_plan, sizeof(RunParams)))) return fail(e, "scratch");
@@ -1457,7 +1364,7 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     // at most 60% of the free memory
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
-    double want = 384.0 * double(hg.arcs) + 64.0 * n;
+    double want = 384.0 * double(g->arcs) + 64.0 * n;
     want = std::max(want, 256.0 * (1 << 20));
     want = std::min(want, 64.0 * (1ull << 30));
     want = std::min(want, 0.6 * double(freeb));
@@ -1465,6 +1372,17 @@ int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
     g->arena_default = g->arena_bytes;
     *out = g;
     return CUTS_OK;
+}
+
+int device_graph_upload(const HostGraph &hg, int device, DeviceGraph **out) {
+    return device_graph_build(hg.n, hg.out_off.data(), hg.out_adj.data(),
+                              hg.symmetric ? nullptr : hg.in_off.data(), hg.symmetric ? nullptr : hg.in_adj.data(),
+                              hg.symmetric ? 1 : 0, false, device, out);
+}
+
+int device_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, const uint64_t *in_off,
+                          const uint32_t *in_adj, int device, DeviceGraph **out) {
+    return device_graph_build(n, out_off, out_adj, in_off, in_adj, -1, true, device, out);
 }
 
 void device_graph_free(DeviceGraph *g) {

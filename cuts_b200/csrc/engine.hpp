@@ -54,6 +54,14 @@ struct DeviceGraph {
 };
 
 int device_graph_upload(const HostGraph &g, int device, DeviceGraph **out);
+// The same from CSR arrays in host memory (validated and checked for
+// symmetry on the device; in-lists may be null for a symmetric graph).
+int device_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, const uint64_t *in_off,
+                          const uint32_t *in_adj, int device, DeviceGraph **out);
+// Builds g's device layout (layout.cu): sym_hint 1 symmetric, 0 directed
+// (in-lists given), -1 decide; validate checks offsets and list order.
+int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, const uint64_t *in_off,
+                  const uint32_t *in_adj, int sym_hint, bool validate, DeviceGraph &g);
 void device_graph_free(DeviceGraph *g);
 
 struct CountResult {

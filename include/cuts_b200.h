@@ -215,7 +215,9 @@ int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count);
 /* Reference in-process API (host_funcs.h:21-25): load both files, make the
  * data graph resident, count, print "<data>,<query>,<ms>ms,<count>" and,
  * when write_to_disk != 0, write ans.txt in the working directory.
- * trunks == 0 runs search(); trunks >= 1 runs search_dfs_bfs_strategy(). */
+ * trunks == 0 runs search(); trunks >= 1 runs search_dfs_bfs_strategy().
+ * The count (every embedding, as the reference's) is found with exact
+ * symmetry breaking unless the environment sets CUTS_PLAIN=1. */
 int cuts_search(const char *query_file, const char *data_file, int write_to_disk,
                 uint32_t trunks, uint64_t *count, float *ms);
 
