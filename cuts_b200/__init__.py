@@ -80,6 +80,7 @@ _SIGS = {
     "cuts_query_set_order": (C.c_int, [_vp, _u32p]),
     "cuts_query_automorphisms": (C.c_int, [_vp, _u64p]),
     "cuts_query_plan_levels": (C.c_int, [_vp, C.c_int, C.c_uint32, _u32p, _u64p]),
+    "cuts_query_prefix": (C.c_int, [_vp, C.c_uint32, C.POINTER(_vp)]),
     "cuts_query_free": (None, [_vp]),
     "cuts_count": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float)]),
     "cuts_count_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _u64p, C.POINTER(C.c_float),
@@ -303,6 +304,13 @@ class Query:
         _check(lib().cuts_plan(self._h, graph._h, mode, model._h if model else None, beam, margin,
                                _ptr(o, _u32p), C.byref(pw), C.byref(sw)))
         return [int(x) for x in o], pw.value, sw.value
+
+    def prefix(self, j: int) -> "Query":
+        """The first j positions of the order as a query whose level sizes are
+        this query's first j level sizes (signatures kept, plain counting)."""
+        h = _vp()
+        _check(lib().cuts_query_prefix(self._h, j, C.byref(h)))
+        return Query(h)
 
     def candidates(self, graph: "Graph", model: "Mlp", count: int = 4, beam: int = 256):
         """The `count` orders with the least predicted work under `model`

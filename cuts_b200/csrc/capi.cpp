@@ -282,6 +282,18 @@ int cuts_query_set_order(cuts_query q, const uint32_t *order) {
     })());
 }
 
+int cuts_query_prefix(cuts_query q, uint32_t j, cuts_query *out) {
+    if (!q || !out) return set_error(CUTS_ERR_ARG, "null argument");
+    *out = nullptr;
+    GUARD(([&]() {
+        auto h = std::make_unique<cuts_query_s>();
+        int rc = query_prefix(q->q, j, h->q);
+        if (rc) return rc;
+        *out = h.release();
+        return CUTS_OK;
+    })());
+}
+
 int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,
                            uint64_t *aut) {
     if (!q || !out) return set_error(CUTS_ERR_ARG, "null argument");

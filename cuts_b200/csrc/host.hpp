@@ -57,6 +57,9 @@ struct Query {
     std::vector<std::vector<uint32_t>> out, in;  // sorted per vertex
     std::vector<uint32_t> order;                 // order[pos] = query vertex
     std::vector<std::vector<uint32_t>> P, C;     // per position: earlier positions
+    // A prefix of a larger query keeps that query's degree signatures and
+    // tests them at every level (empty: the signatures are the degrees here)
+    std::vector<uint32_t> sig_in, sig_out;
     bool has_arc(uint32_t a, uint32_t b) const;
     bool self_loop(uint32_t v) const { return has_arc(v, v); }
     bool loop_free() const;
@@ -71,6 +74,10 @@ int load_query_text(const std::string &path, Query &q);
 // max out-degree, then lexicographic (score1, score2, score3), lowest id on
 // ties) and its P/C lists.
 int score_order(const Query &q, std::vector<uint32_t> &order);
+// The first j positions of q's order as a query of their own (order kept,
+// q's signatures kept): its trie levels are exactly q's first j levels, so
+// their sizes can be logged at a fraction of the full run's cost.
+int query_prefix(const Query &q, uint32_t j, Query &out);
 // Fills q.P / q.C for q.order; rejects orders with an unjoined prefix.
 int set_order(Query &q, const std::vector<uint32_t> &order);
 

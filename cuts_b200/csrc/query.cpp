@@ -136,6 +136,35 @@ int score_order(const Query &q, std::vector<uint32_t> &order) {
     return CUTS_OK;
 }
 
+int query_prefix(const Query &q, uint32_t j, Query &out) {
+    if (q.order.size() != q.k || j < 1 || j > q.k) return set_error(CUTS_ERR_ARG, "bad prefix length");
+    std::vector<int> pos(q.k, -1);
+    for (uint32_t i = 0; i < j; ++i) pos[q.order[i]] = int(i);
+    Query p;
+    p.k = j;
+    p.out.assign(j, {});
+    p.in.assign(j, {});
+    p.sig_in.resize(j);
+    p.sig_out.resize(j);
+    for (uint32_t i = 0; i < j; ++i) {
+        const uint32_t v = q.order[i];
+        for (uint32_t w : q.out[v])
+            if (pos[w] >= 0) p.out[i].push_back(uint32_t(pos[w]));
+        for (uint32_t w : q.in[v])
+            if (pos[w] >= 0) p.in[i].push_back(uint32_t(pos[w]));
+        std::sort(p.out[i].begin(), p.out[i].end());
+        std::sort(p.in[i].begin(), p.in[i].end());
+        p.sig_in[i] = uint32_t(q.in[v].size());
+        p.sig_out[i] = uint32_t(q.out[v].size());
+    }
+    std::vector<uint32_t> ident(j);
+    for (uint32_t i = 0; i < j; ++i) ident[i] = i;
+    int rc = set_order(p, ident);
+    if (rc) return rc;
+    out = std::move(p);
+    return CUTS_OK;
+}
+
 int set_order(Query &q, const std::vector<uint32_t> &order) {
     if (order.size() != q.k) return set_error(CUTS_ERR_ARG, "order length != k");
     std::vector<char> seen(q.k, 0);
@@ -336,8 +365,8 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
     for (uint32_t i = 0; i < k; ++i) {
         LevelPlan &L = plan.lv[i];
         const uint32_t v = q.order[i];
-        L.qin = uint32_t(q.in[v].size());
-        L.qout = uint32_t(q.out[v].size());
+        L.qin = q.sig_in.empty() ? uint32_t(q.in[v].size()) : q.sig_in[v];
+        L.qout = q.sig_out.empty() ? uint32_t(q.out[v].size()) : q.sig_out[v];
         uint32_t nj = 0;
         auto add = [&](uint32_t pos, uint32_t dir) {
             if (data_symmetric) dir = 0;  // in-list == out-list: one list per position
@@ -356,7 +385,7 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
         // candidate that passes the joins and injectivity already has the
         // degrees the signature asks for -- unless the query vertex has a
         // self-loop, which the joins never check but the signature counts.
-        L.check_sig = (i + 1 < k) || q.self_loop(v);
+        L.check_sig = (i + 1 < k) || q.self_loop(v) || !q.sig_in.empty();
         L.closed_form = (k >= 2 && i + 1 == k && nj == 1 && !L.check_sig &&
                          !(flags & CUTS_FLAG_NO_CLOSED_FORM));
         if (L.closed_form) {
@@ -372,9 +401,12 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
             }
         }
     }
-    const bool orbit = (flags & CUTS_FLAG_SYMMETRY_BREAK) && !(flags & CUTS_FLAG_NO_ORBIT_FOLD) &&
-                       q.loop_free() && k >= 3 && orbit_fold_plan(q, data_symmetric, plan);
-    if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && k >= 2 && !orbit) {
+    // symmetry breaking needs the query's own automorphisms, which a prefix
+    // with a larger query's signatures does not have: prefixes count plainly
+    const bool sym = (flags & CUTS_FLAG_SYMMETRY_BREAK) && q.loop_free() && q.sig_in.empty();
+    const bool orbit = sym && !(flags & CUTS_FLAG_NO_ORBIT_FOLD) && k >= 3 &&
+                       orbit_fold_plan(q, data_symmetric, plan);
+    if (sym && k >= 2 && !orbit) {
         std::vector<uint32_t> pos(k);
         for (uint32_t i = 0; i < k; ++i) pos[q.order[i]] = i;
         std::vector<std::pair<uint32_t, uint32_t>> conds;

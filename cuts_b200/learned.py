@@ -63,9 +63,28 @@ def level_sizes(g: "cb.Graph", q: "cb.Query", stride: int, budget_ms: float = 0.
     return [x * max(stride, 1) for x in r.level_sizes], r.ms
 
 
+def prefix_level_sizes(g: "cb.Graph", q: "cb.Query", stride: int, budget_ms: float):
+    """The sizes of q's first levels under its current order: the prefix
+    queries of 2, 3, ... positions (q's signatures kept) are counted on the
+    root stripe until one exceeds budget_ms; returns the longest complete
+    list (at least |L_0|) and the time spent."""
+    best, spent = None, 0.0
+    for j in range(2, q.k + 1):
+        lv, ms = level_sizes(g, q.prefix(j), stride, budget_ms)
+        spent += ms
+        if lv is None:
+            break
+        best = lv
+    return best, spent
+
+
 def collect(g: "cb.Graph", queries: Sequence[Tuple[int, list]], orders_per_query: int = 4,
             stride: int = 1, seed: int = 0, time_budget_s: float = 1e9,
-            run_budget_ms: float = 0.0) -> List[Sample]:
+            run_budget_ms: float = 0.0, prefixes: bool = False) -> List[Sample]:
+    """Per-level sizes of the score order and random orders of each query.
+    With `prefixes`, a run that does not fit run_budget_ms still yields the
+    sizes of the levels its prefixes reach (Sample.levels is then shorter
+    than k)."""
     rng = np.random.default_rng(seed)
     out: List[Sample] = []
     t0 = time.time()
@@ -77,7 +96,10 @@ def collect(g: "cb.Graph", queries: Sequence[Tuple[int, list]], orders_per_query
         orders = [score] + [random_order(k, arcs, rng) for _ in range(orders_per_query - 1)]
         for j, o in enumerate(orders):
             q.set_order(o)
-            lv, ms = level_sizes(g, q, stride, run_budget_ms)
+            if prefixes:
+                lv, ms = prefix_level_sizes(g, q, stride, run_budget_ms)
+            else:
+                lv, ms = level_sizes(g, q, stride, run_budget_ms)
             if lv is None:  # too expensive to log within the run budget
                 continue
             out.append(Sample(qi, list(o), lv, ms, j == 0))
@@ -93,10 +115,12 @@ def features(g: "cb.Graph", queries, samples: Sequence[Sample]):
             k, arcs = queries[s.query]
             cache[s.query] = cb.Query.from_arcs(k, arcs)
         q = cache[s.query]
-        F = q.features(g, s.order, s.levels)
+        n = len(s.levels)  # a prefix run logs the first n levels only
+        lv = list(s.levels) + [0] * (q.k - n)
+        F = q.features(g, s.order, lv)[:n]
         X.append(F)
         y.append(np.log1p(np.array(s.levels, np.float64)).astype(np.float32))
-        qid += [s.query] * len(s.levels)
+        qid += [s.query] * n
     return np.concatenate(X), np.concatenate(y), np.array(qid)
 
 

@@ -86,7 +86,7 @@ def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, s
     train_q = eval_queries(n_train, seed0=seed)
     t0 = time.perf_counter()
     samples = L.collect(g, train_q, orders_per_query=orders_per_query, stride=stride, seed=1,
-                        time_budget_s=time_budget_s, run_budget_ms=run_budget_ms)
+                        time_budget_s=time_budget_s, run_budget_ms=run_budget_ms, prefixes=True)
     t_collect = time.perf_counter() - t0
     _log(f"training data: {len(samples)} runs in {t_collect:.1f} s")
     X, y, _ = L.features(g, train_q, samples)
@@ -94,6 +94,7 @@ def train_model(g: "cb.Graph", n_train: int = 2000, orders_per_query: int = 4, s
     model = L.train(X, y, epochs=epochs, batch=4096, lr=2e-3)
     t_train = time.perf_counter() - t1
     info = {"samples": len(samples), "queries_logged": len({s.query for s in samples}),
+            "complete_runs": sum(1 for s in samples if len(s.levels) == train_q[s.query][0]),
             "rows": int(len(y)), "collect_s": t_collect, "train_s": t_train,
             "fit_mae_nats": L.prediction_error(model, X, y)}
     _log(f"model: {info}")

@@ -143,6 +143,14 @@ int cuts_query_joins(cuts_query q, uint32_t *p_off, uint32_t *p, uint32_t *c_off
 /* Replace the order (a permutation whose every prefix is connected). */
 int cuts_query_set_order(cuts_query q, const uint32_t *order);
 
+/* The first j positions of q's matching order as a query of its own (a
+ * new handle, freed with cuts_query_free): it keeps q's degree signatures,
+ * tests them at every level and counts plainly (no symmetry breaking), so its
+ * per-level sizes are exactly the sizes of q's first j trie levels -- the
+ * cheap way to log them when q's full count is out of reach.  No reference
+ * counterpart. */
+int cuts_query_prefix(cuts_query q, uint32_t j, cuts_query *out);
+
 /* The per-level plan the kernels run for the current order, for a data
  * graph that is symmetric or not and the given flags: 11 words per level,
  * {joined lists, signature test, closed form, folded into the level before,

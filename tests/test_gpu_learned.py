@@ -102,3 +102,23 @@ def test_candidates_and_measured_choice(setup):
         assert g.count(q).count == want
         if times[tuple(score)] is not None and tuple(order) != tuple(score):
             assert times[tuple(order)] < times[tuple(score)]
+
+
+def test_prefix_levels_equal_full_levels(setup):
+    """The prefix queries' level sizes are the full query's first levels
+    (oracle), and the prefix logger returns them."""
+    from oracle import oracle as O
+    from tests.helpers import oracle_graph_from_host
+    h = cb.HostGraph.chung_lu(3000, 12000, 2.2, 2.0, 60.0, seed=8)
+    g = h.upload(0)
+    od = oracle_graph_from_host(h)
+    for s in range(6):
+        k = 4 + s % 3
+        arcs = cb.random_query_arcs(k, 0.3, 500 + s)
+        q = cb.Query.from_arcs(k, arcs)
+        _, want, _ = O.count(od, O.Graph.from_arcs(k, arcs), q.order)
+        for j in range(2, k + 1):
+            r = g.count(q.prefix(j), stats=True)
+            assert r.level_sizes == list(want[:j]), (s, j)
+        lv, _ = L.prefix_level_sizes(g, q, 1, 0.0)
+        assert lv == list(want)

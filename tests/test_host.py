@@ -403,3 +403,23 @@ def test_orbit_fold_plan_shape():
     # without symmetry breaking: the plain fold, no orbit
     lv0, aut0 = q.plan_levels(True, 0)
     assert lv0[k - 1]["ofold"] == 0 and aut0 == 1
+
+
+def test_query_prefix_keeps_the_first_levels_plan():
+    """A prefix query's plan is the full plan's first j levels: same joins and
+    signatures, the signature tested at every level, no closed form."""
+    for k, arcs in [cb.named_query_arcs("house"), cb.named_query_arcs("4-clique+pendant"),
+                    (6, cb.random_query_arcs(6, 0.3, 3)), (5, [(0, 1), (1, 2), (2, 0), (0, 3), (3, 4)])]:
+        q = cb.Query.from_arcs(k, arcs)
+        full, _ = q.plan_levels(True, 0)
+        for j in range(1, k + 1):
+            p = q.prefix(j)
+            assert p.k == j and p.order == list(range(j))
+            lv, aut = p.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)  # prefixes count plainly
+            assert aut == 1
+            for i in range(j):
+                for key in ("joins", "qin", "qout", "gt", "lt"):
+                    assert lv[i][key] == (full[i][key] if key not in ("gt", "lt") else 0), (k, j, i, key)
+                assert lv[i]["sig"] == 1 and lv[i]["closed"] == 0 and lv[i]["ofold"] == 0
+    with pytest.raises(cb.CutsError):
+        q.prefix(0)
