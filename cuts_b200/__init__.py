@@ -101,6 +101,7 @@ _SIGS = {
     "cuts_batch_run": (C.c_int, [_vp, C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "cuts_batch_info": (C.c_int, [_vp, _u64p, _u32p]),
     "cuts_batch_set_query_budget": (C.c_int, [_vp, C.c_double]),
+    "cuts_batch_set_shard": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "cuts_plan_candidates": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint32, _u32p,
                                        C.POINTER(C.c_double), _u32p]),
     "cuts_batch_free": (None, [_vp]),
@@ -581,6 +582,10 @@ class Batch:
         """Each query may use `ms` of the whole GPU in later runs; a query past
         it reports ERR_BUDGET while the others carry on (0 = no limit)."""
         _check(lib().cuts_batch_set_query_budget(self._h, ms))
+
+    def set_shard(self, shard: int, nshards: int) -> None:
+        """Later runs take the tasks t % nshards == shard only (one GPU's part)."""
+        _check(lib().cuts_batch_set_shard(self._h, shard, nshards))
 
     def info(self):
         t, b = C.c_uint64(), C.c_uint32()

@@ -212,23 +212,26 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
         unsigned long long *__restrict__ task_ctr, uint32_t *__restrict__ stop,
         unsigned long long *__restrict__ counts, uint32_t *__restrict__ aborted,
         unsigned long long budget_ns, unsigned long long *__restrict__ qtime,
-        unsigned long long qlimit) {
+        unsigned long long qlimit, uint32_t shard, uint32_t nshards) {
     __shared__ BWarp ws[kBW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Ctx c{g, nullptr, &ws[warp], lane};
     const unsigned long long total = qbase[nq];
+    // this shard's tasks are t = c * nshards + shard for counter values c
+    const unsigned long long ctotal = total > shard ? (total - shard + nshards - 1) / nshards : 0;
     const unsigned long long deadline = budget_ns ? global_ns() + budget_ns : ~0ull;
     uint32_t cur = kFullMask;
     unsigned long long qcount = 0;
     volatile uint32_t *vstop = stop;
 
     while (true) {
-        unsigned long long t0 = 0;
-        if (lane == 0) t0 = *vstop ? total : atomicAdd(task_ctr, (unsigned long long)tgrab);
-        t0 = __shfl_sync(kFullMask, t0, 0);
-        if (t0 >= total) break;
-        const unsigned long long t1 = min(t0 + tgrab, total);
-        for (unsigned long long t = t0; t < t1; ++t) {
+        unsigned long long c0 = 0;
+        if (lane == 0) c0 = *vstop ? ctotal : atomicAdd(task_ctr, (unsigned long long)tgrab);
+        c0 = __shfl_sync(kFullMask, c0, 0);
+        if (c0 >= ctotal) break;
+        const unsigned long long c1 = min(c0 + tgrab, ctotal);
+        for (unsigned long long cc = c0; cc < c1; ++cc) {
+            const unsigned long long t = cc * nshards + shard;
             if (cur == kFullMask || t < qbase[cur] || t >= qbase[cur + 1]) {
                 if (cur != kFullMask && lane == 0 && qcount) atomicAdd(&counts[cur], qcount);
                 qcount = 0;
@@ -253,7 +256,8 @@ k_batch(DevView g, const BQuery *__restrict__ qs, uint32_t nq,
                            reinterpret_cast<volatile unsigned long long *>(qtime)[cur] > qlimit;
                     if (skip) {
                         aborted[cur] = 1;
-                        atomicMax(task_ctr, qbase[cur + 1]);
+                        const unsigned long long e = qbase[cur + 1];
+                        atomicMax(task_ctr, e > shard ? (e - shard + nshards - 1) / nshards : 0ull);
                     }
                 }
                 if (__shfl_sync(kFullMask, skip, 0)) continue;
@@ -495,7 +499,9 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
 }
 
 int Batch::capture(unsigned long long budget_ns) {
-    if (exec && budget_ns == captured_budget && query_budget_ms == captured_query_budget) return CUTS_OK;
+    if (exec && budget_ns == captured_budget && query_budget_ms == captured_query_budget &&
+        shard == captured_shard && nshards == captured_nshards)
+        return CUTS_OK;
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
     if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
     int bps = 0;
@@ -503,7 +509,7 @@ int Batch::capture(unsigned long long budget_ns) {
     int sms = 0;
     BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
     if (tune.blocks_per_sm) bps = std::min<int>(bps, int(tune.blocks_per_sm));
-    const unsigned long long maxb = (total_tasks + kBW - 1) / kBW;
+    const unsigned long long maxb = (total_tasks / std::max<uint32_t>(nshards, 1) + kBW) / kBW;
     const uint32_t blocks = uint32_t(std::max<unsigned long long>(1, std::min<unsigned long long>(
         (unsigned long long)(std::max(1, bps) * sms), maxb)));
     const unsigned long long *pref = g->batch_pref;
@@ -521,7 +527,7 @@ int Batch::capture(unsigned long long budget_ns) {
             DevView{g->out_info, g->in_info, g->adj, g->n}, d_queries, nb, d_qbase, g->batch_vsorted,
             pref, g->symmetric ? pref : pref + stride, g->symmetric ? pref : pref + 2 * stride, tune.grain,
             tune.tasks_per_grab, d_ctr, reinterpret_cast<uint32_t *>(d_ctr + 1), d_counts, d_aborted,
-            budget_ns, d_qtime, qlimit);
+            budget_ns, d_qtime, qlimit, shard, nshards);
     }
     cudaMemcpyAsync(h_counts, d_counts, sizeof(unsigned long long) * std::max<uint32_t>(nb, 1),
                     cudaMemcpyDeviceToHost, s);
@@ -534,6 +540,8 @@ int Batch::capture(unsigned long long budget_ns) {
     BCK(cudaGraphInstantiate(&exec, graph, 0));
     captured_budget = budget_ns;
     captured_query_budget = query_budget_ms;
+    captured_shard = shard;
+    captured_nshards = nshards;
     launch_blocks = blocks;
     return CUTS_OK;
 }
@@ -551,7 +559,8 @@ int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int>
     BCK(cudaStreamSynchronize(g->stream));
     float t = 0;
     BCK(cudaEventElapsedTime(&t, g->ev0, g->ev1));
-    const unsigned long long stop_at = std::min<unsigned long long>(h_ctr[0], total_tasks);
+    // tasks below stop_at were all taken (counter values map to c * nshards + shard)
+    const unsigned long long stop_at = std::min<unsigned long long>(h_ctr[0] * nshards + shard, total_tasks);
     const bool stopped = reinterpret_cast<uint32_t *>(h_ctr + 1)[0] != 0;
     for (uint32_t b = 0; b < nb; ++b) {
         const uint32_t i = index[b];
@@ -566,6 +575,8 @@ int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int>
         CountOptions opt;
         opt.flags = flags;
         opt.budget_ms = query_budget_ms;
+        opt.shard = shard;
+        opt.nshards = nshards;
         rc = device_count(*g, *queries[i], opt, r);
         if (rc) {
             status[i] = rc;

@@ -60,6 +60,8 @@ struct Batch {
     cudaGraphExec_t exec = nullptr;
     unsigned long long captured_budget = ~0ull;
     double captured_query_budget = -1;
+    uint32_t shard = 0, nshards = 1;  // tasks t with t % nshards == shard (one GPU of several)
+    uint32_t captured_shard = 0, captured_nshards = 0;
     uint32_t launch_blocks = 0;
 
     int create(DeviceGraph &g, const std::vector<const Query *> &qs, uint32_t flags,
@@ -71,6 +73,9 @@ struct Batch {
     // summed over the launch's warps, up to query_budget_ms x warps); a query
     // past it reports CUTS_ERR_BUDGET and the others carry on.  0 = no limit.
     void set_query_budget(double ms) { query_budget_ms = ms; }
+    // This launch takes only the tasks t with t % nshards == shard, so
+    // nshards launches (one per GPU) partition every query's count.
+    void set_shard(uint32_t s, uint32_t n) { shard = s; nshards = n; }
     void destroy();
 
   private:

@@ -606,6 +606,12 @@ int cuts_batch_set_query_budget(cuts_batch b, double ms) {
     return CUTS_OK;
 }
 
+int cuts_batch_set_shard(cuts_batch b, uint32_t shard, uint32_t nshards) {
+    if (!b || nshards == 0 || shard >= nshards) return set_error(CUTS_ERR_ARG, "bad batch or shard");
+    b->b.set_shard(shard, nshards);
+    return CUTS_OK;
+}
+
 int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks) {
     if (!b) return set_error(CUTS_ERR_ARG, "null batch");
     if (tasks) *tasks = b->b.total_tasks;

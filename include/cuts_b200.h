@@ -300,6 +300,12 @@ int cuts_batch_run(cuts_batch b, double budget_ms, uint64_t *counts, int *status
  * carry on.  0 = no limit (the default).  No reference counterpart: the
  * reference runs one query per process. */
 int cuts_batch_set_query_budget(cuts_batch b, double ms);
+/* Later cuts_batch_run calls take only the tasks t with t % nshards == shard
+ * (tasks are (query, root, level-1 range)), so one launch per GPU with
+ * shard = rank partitions every query's count; sum the per-query counts over
+ * ranks.  Plays the part of the reference's rank striping of roots
+ * (device_funcs.cu:273, main_mpi.cu) for a batch. */
+int cuts_batch_set_shard(cuts_batch b, uint32_t shard, uint32_t nshards);
 int cuts_batch_info(cuts_batch b, uint64_t *tasks, uint32_t *blocks);
 void cuts_batch_free(cuts_batch b);
 

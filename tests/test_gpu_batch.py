@@ -158,3 +158,25 @@ def test_batch_query_budget_drops_only_the_heavy_query():
     b2 = g.batch(cheap)
     c2, s2, _ = b2.run()
     assert s2 == [0, 0, 0] and c2 == counts[1:]
+
+
+def test_batch_shards_partition_every_query():
+    """One launch per shard (as one per GPU): the per-query counts of the
+    shards add up to the unsharded counts, for every shard count."""
+    h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
+    g = h.upload(0)
+    qs = [cb.Query.from_arcs(*cb.named_query_arcs(n)) for n in ("triangle", "4-cycle", "house", "4-clique+pendant")]
+    qs += [cb.Query.from_arcs(k, cb.random_query_arcs(k, 0.4, 70 + k)) for k in (3, 4, 5)]
+    full, st, _ = g.batch(qs).run()
+    assert st == [0] * len(qs)
+    for nshards in (2, 3, 7):
+        tot = [0] * len(qs)
+        for r in range(nshards):
+            b = g.batch(qs)
+            b.set_shard(r, nshards)
+            c, s, _ = b.run()
+            assert s == [0] * len(qs)
+            tot = [a + x for a, x in zip(tot, c)]
+        assert tot == full
+    with pytest.raises(cb.CutsError):
+        g.batch(qs).set_shard(3, 3)
