@@ -123,13 +123,15 @@ def estimate_orders(g: "cb.Graph", qdefs, orders_a, orders_b, stride: int, budge
 
 def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms: float = 100.0,
                 model=None, train_budget_s: float = 120.0, flags: int = 0,
-                est_stride: int = 1 << 12, est_budget_ms: float = 300.0):
+                est_stride: int = 1 << 12, est_budget_ms: float = 300.0,
+                choose_stride: int = 1 << 14, choose_budget_ms: float = 100.0):
     """The 200 evaluation queries three ways, each query under the same
     budget of budget_ms of the whole GPU:
       plain    -- score order, level engine, one query at a time;
       learned  -- the learned order (the model's three best proposals and the
-                  score order timed on a small root stripe, the fastest
-                  kept), level engine, one query at a time;
+                  score order timed on a root stripe of 1/choose_stride of
+                  the roots, the fastest kept), level engine, one query at a
+                  time;
       learned_batched -- the learned order, all queries in one persistent
                   launch (cheapest measured first), each limited to
                   budget_ms of GPU time by the batched kernel's per-query limit.
@@ -152,7 +154,8 @@ def run_learned(g: "cb.Graph", n_eval: int = 200, n_train: int = 2000, budget_ms
         model_switched += pw < sw
         q.set_order(score)
         # the model's proposals, measured on a small root stripe (shard 0)
-        order, times = L.choose_order(g, q, model, proposals=3, flags=flags)
+        order, times = L.choose_order(g, q, model, proposals=3, stride=choose_stride,
+                                      budget_ms=choose_budget_ms, flags=flags)
         switched += order != score
         qs.append(q)
         t = times.get(tuple(order))
