@@ -211,8 +211,8 @@ int cuts_graph_set_arena_bytes(cuts_graph g, uint64_t bytes) {
     if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
     DeviceGraph &d = *g->dev;
     cudaSetDevice(d.device);
+    if (d.arena) cudaFreeAsync(d.arena, d.stream);
     cudaStreamSynchronize(d.stream);
-    cudaFree(d.arena);
     d.arena = nullptr;
     d.arena_bytes = bytes ? size_t(bytes) : d.arena_default;
     return CUTS_OK;

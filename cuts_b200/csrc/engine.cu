@@ -1347,6 +1347,16 @@ static int device_graph_build(uint32_t n, const uint64_t *out_off, const uint32_
     };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking))) return fail(e, "stream");
+    {
+        // the trie arena and the layout's scratch come from the device's
+        // default pool; keep up to 32 GB of freed blocks there, so a graph
+        // built after another one reuses its memory instead of mapping anew
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = 32ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     int rc = device_layout(n, out_off, out_adj, in_off, in_adj, sym_hint, validate, *g);
     if (rc) {
         device_graph_free(g);
@@ -1388,11 +1398,11 @@ int device_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *o
 void device_graph_free(DeviceGraph *g) {
     if (!g) return;
     cudaSetDevice(g->device);
+    if (g->arena && g->stream) cudaFreeAsync(g->arena, g->stream);  // back to the pool
     if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->in_info && g->in_info != g->out_info) cudaFree(g->in_info);
     cudaFree(g->out_info);
     cudaFree(g->adj);
-    cudaFree(g->arena);
     cudaFree(g->d_u32);
     cudaFree(g->d_u64);
     cudaFree(g->d_plan);
@@ -1705,7 +1715,7 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     if (fuse) stored = cl - 1;
     hp->stored = stored;
     if (!g.arena) {
-        cudaError_t e = cudaMalloc(&g.arena, g.arena_bytes);
+        cudaError_t e = cudaMallocAsync(&g.arena, g.arena_bytes, g.stream);
         if (e != cudaSuccess) {
             g.arena = nullptr;
             return set_error(CUTS_ERR_NOMEM, "arena allocation failed: " + std::string(cudaGetErrorString(e)));

@@ -160,17 +160,22 @@ __global__ void k_loops(uint32_t n, const uint2 *__restrict__ info, const uint32
     }
 }
 
-// Device buffers of one build, released on every exit.
+// Device buffers of one build, stream-ordered from the device's memory pool
+// (reused across builds instead of mapped and unmapped each time), released
+// on every exit.
 struct Scratch {
+    cudaStream_t s;
     std::vector<void *> p;
+    explicit Scratch(cudaStream_t st) : s(st) {}
     ~Scratch() {
-        for (void *x : p) cudaFree(x);
+        for (void *x : p) cudaFreeAsync(x, s);
+        cudaStreamSynchronize(s);
     }
     template <class T>
     cudaError_t get(T **out, size_t count) {
         *out = nullptr;
         if (!count) count = 1;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void **>(out), sizeof(T) * count);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(out), sizeof(T) * count, s);
         if (e == cudaSuccess) p.push_back(*out);
         return e;
     }
@@ -195,7 +200,7 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     if (in_off && in_off[n] != m) return set_error(CUTS_ERR_ARG, "in/out arc counts differ");
     cudaStream_t s = g.stream;
     const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, 148u * 16));
-    Scratch sc;
+    Scratch sc(s);
     uint64_t *d_ooff = nullptr, *d_ioff = nullptr;
     uint32_t *d_oadj = nullptr, *d_iadj = nullptr, *d_flag = nullptr;
     LCK(sc.get(&d_ooff, size_t(n) + 1));
