@@ -594,7 +594,7 @@ int Batch::run(double budget_ms, std::vector<uint64_t> &counts, std::vector<int>
 //
 // For callers that may not allocate GPU memory themselves: code running inside
 // a host framework that owns every device allocation (a memory pool that must
-// account for all bytes, a capture-only execution model, a plugin sandbox).
+// account for all bytes, a plugin sandbox).
 // They pass the graph and the output buffer they already own; the engine's
 // own scratch for this path -- the per-query plans and the work counter --
 // lives in the fixed array below, which every GPU that loads this library
@@ -618,6 +618,27 @@ constexpr int kNoAllocMaxDevices = 64;
 NoAllocScratch *g_noalloc_ptr[kNoAllocMaxDevices] = {};
 uint32_t g_noalloc_blocks[kNoAllocMaxDevices] = {};
 std::mutex g_noalloc_mutex;
+
+// The query plans travel as kernel parameters, copied into the scratch array
+// by a one-block kernel: the launch records them by value when it is queued,
+// so the call needs no host staging buffer and returns without waiting.
+constexpr uint32_t kNoAllocPlansPerLaunch = 16;  // 16 x 656 B of parameters
+struct NoAllocPlans {
+    BQuery q[kNoAllocPlansPerLaunch];
+};
+
+__global__ void k_noalloc_plans(const NoAllocPlans plans, uint32_t first, uint32_t count,
+                                NoAllocScratch *__restrict__ sc) {
+    const uint32_t words = count * uint32_t(sizeof(BQuery) / 4);
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(plans.q);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(sc->queries + first);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+    // the work counter and the stop flag start at zero
+    if (first == 0 && threadIdx.x == 0) {
+        sc->task_ctr = 0;
+        sc->stop = 0;
+    }
+}
 
 // Tasks are (query, root vertex) pairs in vertex-id order, query-major; each
 // runs the root's whole level-1 list depth first with the same level steps as
@@ -687,8 +708,8 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
         return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: more than 64 queries in one call");
     if (flags & CUTS_FLAG_SYMMETRY_BREAK)
         return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: symmetry breaking is not available here");
-    // host copy of the query table: on the stack, fixed size, no allocation
-    BQuery table[kNoAllocMaxQueries];
+    // the query plans, built on the stack (fixed size, no allocation)
+    NoAllocPlans table[kNoAllocMaxQueries / kNoAllocPlansPerLaunch];
     const bool sym = symmetric != 0 || info_in == nullptr;
     for (uint32_t i = 0; i < nq; ++i) {
         if (!qs[i]) return set_error(CUTS_ERR_ARG, "cuts_count_noalloc: null query");
@@ -698,7 +719,7 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
         Plan plan;
         int rc = build_plan(q, sym, flags | CUTS_FLAG_NO_ORBIT_FOLD, plan);  // plain fold only
         if (rc) return rc;
-        BQuery &b = table[i];
+        BQuery &b = table[i / kNoAllocPlansPerLaunch].q[i % kNoAllocPlansPerLaunch];
         std::memset(&b, 0, sizeof(b));
         b.k = q.k;
         for (uint32_t d = 0; d < q.k; ++d) {
@@ -744,13 +765,18 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
         sc = g_noalloc_ptr[dev];
         blocks = g_noalloc_blocks[dev];
     }
-    // counts and the work counter start at zero on every call
-    if (cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * std::max<uint32_t>(nq, 1), stream) != cudaSuccess ||
-        cudaMemsetAsync(&sc->task_ctr, 0, sizeof(unsigned long long) + sizeof(uint32_t), stream) != cudaSuccess)
+    // nothing to count: the caller's counts buffer (nq entries) is not touched
+    if (nq == 0) return CUTS_OK;
+    // counts start at zero on every call
+    if (cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * nq, stream) != cudaSuccess)
         return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: memset failed");
-    if (nq == 0 || n == 0) return CUTS_OK;
-    if (cudaMemcpyAsync(sc->queries, table, sizeof(BQuery) * nq, cudaMemcpyHostToDevice, stream) != cudaSuccess)
-        return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: plan upload failed");
+    if (n == 0) return CUTS_OK;
+    for (uint32_t first = 0; first < nq; first += kNoAllocPlansPerLaunch) {
+        const uint32_t cnt = std::min(kNoAllocPlansPerLaunch, nq - first);
+        k_noalloc_plans<<<1, 256, 0, stream>>>(table[first / kNoAllocPlansPerLaunch], first, cnt, sc);
+        if (cudaGetLastError() != cudaSuccess)
+            return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: plan upload failed");
+    }
     const DevView view{reinterpret_cast<const uint2 *>(info_out),
                        reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n};
     const unsigned long long total = (unsigned long long)nq * n;

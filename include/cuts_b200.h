@@ -200,6 +200,12 @@ int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t fla
                        uint32_t shard, uint32_t nshards, uint64_t *count, float *ms,
                        uint64_t *level_sizes);
 
+/* cuts_count_sharded with the statistics of cuts_count_ex (stats[8], same
+ * layout and the same opt-in entries). */
+int cuts_count_sharded_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags,
+                          uint32_t shard, uint32_t nshards, uint64_t *count, float *ms,
+                          uint64_t *level_sizes, uint64_t *stats);
+
 /* As cuts_count, but stops with CUTS_ERR_BUDGET once budget_ms has passed:
  * the host checks between chunks, and every kernel of the run stops taking
  * work once budget_ms of device time has passed since the run's first
@@ -316,12 +322,19 @@ void cuts_batch_free(cuts_batch b);
  * account for all bytes, a sandboxed plugin): count up to 64 queries in one
  * launch using only buffers the caller passes in.  No reference counterpart.
  *
- * Inputs, in the caller's device memory: info_out[2v] = offset of v's sorted
+ * Inputs, in the caller's device memory: info_out[2v] = offset of v's
  * out-list in adj, info_out[2v+1] = its length (u32 pairs, 8-byte aligned);
  * info_in likewise for in-lists, or NULL for a symmetric graph; adj (u32).
+ * The caller guarantees what the resident-graph path validates on upload:
+ * every list strictly increasing (sorted, no duplicates), every id below n,
+ * every (offset, length) inside adj, and for info_in == NULL every arc's
+ * reverse present.  These are not checked here: duplicates give wrong
+ * counts and out-of-range ids read out of bounds.
  * Output: counts[nq] (u64, device memory), overwritten with the exact count
- * of each query.  Work is queued on `stream` (a cudaStream_t, NULL = the
- * default stream) and the call returns without waiting; synchronise the
+ * of each query (not touched when nq == 0; zeros when n == 0).  Work is
+ * queued on `stream` (a cudaStream_t, NULL = the default stream) and the
+ * call returns without waiting: the query plans travel as kernel
+ * parameters, so no host buffer has to outlive the call.  Synchronise the
  * stream before reading counts.
  *
  * Calls no cudaMalloc, cudaFree or other allocating routine.  The engine's
