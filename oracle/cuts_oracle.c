@@ -18,6 +18,7 @@
 #include <ctype.h>
 #include <errno.h>
 #include <limits.h>
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -257,6 +258,13 @@ typedef struct {
     uint32_t jpos[OR_MAX_QUERY][2 * OR_MAX_QUERY];
     uint8_t jout[OR_MAX_QUERY][2 * OR_MAX_QUERY];     /* 1 = P join (out-list) */
     int symmetric;
+    /* ordering conditions: at level i the candidate must exceed M[j] for
+     * j in gt[i] and lie below M[j] for j in lt[i] (0 = no condition) */
+    uint32_t gt[OR_MAX_QUERY], lt[OR_MAX_QUERY];
+    /* count the last level by list arithmetic when it joins one list */
+    int closed_last;
+    int last_single;      /* the last level's joins name one list */
+    int last_loop_free;   /* the last query vertex has no self-loop */
 } plan_t;
 
 typedef struct {
@@ -313,6 +321,25 @@ static void emit(const plan_t *P, acc_t *A, const uint32_t *M) {
     A->cb(by_q, P->k, A->user);
 }
 
+static uint64_t lower_bound_u32(const uint32_t *a, uint64_t len, uint32_t x) {
+    uint64_t lo = 0, hi = len;
+    while (lo < hi) {
+        uint64_t m = lo + (hi - lo) / 2;
+        if (a[m] < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+/* Candidate window [lo, hi) of level i from the ordering conditions. */
+static void cond_window(const plan_t *P, uint32_t i, const uint32_t *M, uint32_t *lo, uint32_t *hi) {
+    uint32_t a = 0, b = UINT32_MAX;
+    for (uint32_t j = 0; j < i; ++j) {
+        if (((P->gt[i] >> j) & 1u) && M[j] + 1 > a) a = M[j] + 1;
+        if (((P->lt[i] >> j) & 1u) && M[j] < b) b = M[j];
+    }
+    *lo = a; *hi = b;
+}
+
 /* Expand the partial match M[0..i-1] at level i. */
 static void extend(const plan_t *P, acc_t *A, uint32_t i, uint32_t *M) {
     A->bytes += parent_bytes(P, i, M);
@@ -324,8 +351,26 @@ static void extend(const plan_t *P, acc_t *A, uint32_t i, uint32_t *M) {
         list_of(P, i, t, M, &l, &len);
         if (len < blen) { blen = len; best = t; bl = l; }
     }
+    uint32_t lo = 0, hi = UINT32_MAX;
+    if (P->gt[i] | P->lt[i]) cond_window(P, i, M, &lo, &hi);
+    if (P->closed_last && i + 1 == P->k && P->last_single && P->last_loop_free && !A->cb) {
+        /* one list, every query neighbour of the last vertex already
+         * matched: each list element in the window that is not matched yet
+         * extends (the joins imply the signature) */
+        uint64_t s0 = lo ? lower_bound_u32(bl, blen, lo) : 0;
+        uint64_t e0 = hi != UINT32_MAX ? lower_bound_u32(bl, blen, hi) : blen;
+        if (e0 > s0) {
+            uint64_t c = e0 - s0;
+            for (uint32_t j = 0; j < i; ++j)
+                if (M[j] >= lo && M[j] < hi && bsearch_u32(bl, 0, blen, M[j])) --c;
+            A->lvl[i] += c;
+        }
+        return;
+    }
     for (uint64_t x = 0; x < blen; ++x) {
         uint32_t c = bl[x];
+        if (c < lo) continue;
+        if (c >= hi) break;
         int used = 0;
         for (uint32_t j = 0; j < i; ++j) if (M[j] == c) { used = 1; break; }
         if (used || !sig_ok(P, i, c)) continue;
@@ -378,36 +423,62 @@ static int make_plan(const or_graph *d, const or_graph *q, const uint32_t *order
          * for disconnected queries, which the oracle rejects */
         if (i > 0 && n == 0) return OR_ERR_QUERY;
     }
+    {
+        uint32_t i = k - 1, v = order[i];
+        P->last_single = k >= 2;
+        for (uint32_t t = 1; t < P->nj[i]; ++t) {
+            int same = P->jpos[i][t] == P->jpos[i][0] && (P->symmetric || P->jout[i][t] == P->jout[i][0]);
+            if (!same) P->last_single = 0;
+        }
+        P->last_loop_free = !lin_has(v, q->out_adj, q->out_off[v], q->out_off[v + 1]);
+    }
     return OR_OK;
 }
 
 static int count_impl(const or_graph *d, const or_graph *q, const uint32_t *order_in,
                       uint32_t root_begin, uint32_t root_end, uint32_t shard, uint32_t nshards,
+                      const uint32_t *conds, uint32_t ncond, uint32_t opts,
                       int nthreads, uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes);
 
 int or_count(const or_graph *d, const or_graph *q, const uint32_t *order_in,
              uint32_t root_begin, uint32_t root_end, int nthreads,
              uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes) {
-    return count_impl(d, q, order_in, root_begin, root_end, 0, 1, nthreads, count, level_sizes,
-                      alg_bytes);
+    return count_impl(d, q, order_in, root_begin, root_end, 0, 1, NULL, 0, 0, nthreads, count,
+                      level_sizes, alg_bytes);
 }
 
 int or_count_striped(const or_graph *d, const or_graph *q, const uint32_t *order,
                      uint32_t shard, uint32_t nshards, int nthreads, uint64_t *count,
                      uint64_t *level_sizes) {
     if (nshards == 0 || shard >= nshards) return OR_ERR_QUERY;
-    return count_impl(d, q, order, 0, UINT32_MAX, shard, nshards, nthreads, count, level_sizes,
-                      NULL);
+    return count_impl(d, q, order, 0, UINT32_MAX, shard, nshards, NULL, 0, 0, nthreads, count,
+                      level_sizes, NULL);
+}
+
+int or_count_ex(const or_graph *d, const or_graph *q, const uint32_t *order,
+                const uint32_t *conds, uint32_t ncond, uint32_t shard, uint32_t nshards,
+                uint32_t opts, int nthreads, uint64_t *count, uint64_t *level_sizes) {
+    if (nshards == 0 || shard >= nshards) return OR_ERR_QUERY;
+    if (ncond && !conds) return OR_ERR_QUERY;
+    return count_impl(d, q, order, 0, UINT32_MAX, shard, nshards, conds, ncond, opts, nthreads,
+                      count, level_sizes, NULL);
 }
 
 static int count_impl(const or_graph *d, const or_graph *q, const uint32_t *order_in,
                       uint32_t root_begin, uint32_t root_end, uint32_t shard, uint32_t nshards,
+                      const uint32_t *conds, uint32_t ncond, uint32_t opts,
                       int nthreads, uint64_t *count, uint64_t *level_sizes, uint64_t *alg_bytes) {
     plan_t P;
     uint32_t order[OR_MAX_QUERY];
     int rc = make_plan(d, q, order_in, &P, order);
     if (rc) return rc;
     uint32_t k = P.k;
+    for (uint32_t c = 0; c < ncond; ++c) {  /* M[a] < M[b], checked at the later position */
+        uint32_t a = conds[2 * c], b = conds[2 * c + 1];
+        if (a >= k || b >= k || a == b) return OR_ERR_QUERY;
+        if (a < b) P.gt[b] |= 1u << a; else P.lt[a] |= 1u << b;
+    }
+    P.closed_last = (opts & OR_OPT_CLOSED_LAST) != 0;
     /* level 0 (device_funcs.cu:267-279), in vertex-id order */
     uint32_t *roots = (uint32_t *)malloc(((size_t)d->n + 1) * sizeof(uint32_t));
     if (!roots) return OR_ERR_NOMEM;
@@ -469,4 +540,144 @@ int or_enumerate(const or_graph *d, const or_graph *q, const uint32_t *order_in,
         extend(&P, &A, 1, M);
     }
     return OR_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* seeded Chung-Lu generator and degree relabelling                    */
+/* ------------------------------------------------------------------ */
+
+/* splitmix64 (Steele, Lea & Flood 2014) */
+static uint64_t sm64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static double unit_open(uint64_t h) { return (double)((h >> 11) + 1) * (1.0 / 9007199254740993.0); }
+
+typedef struct {
+    float *prob;
+    uint32_t *alias;
+    uint32_t n;
+} alias_t;
+
+/* Vose's alias method over weights w[0..n) (double arithmetic, float
+ * probabilities, LIFO work lists). */
+static int alias_build(const double *w, uint32_t n, alias_t *A) {
+    A->n = n;
+    A->prob = (float *)calloc(n, sizeof(float));
+    A->alias = (uint32_t *)calloc(n, sizeof(uint32_t));
+    double *sc = (double *)malloc((size_t)n * sizeof(double));
+    uint32_t *small = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    uint32_t *large = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    if (!A->prob || !A->alias || !sc || !small || !large) {
+        free(A->prob); free(A->alias); free(sc); free(small); free(large);
+        return OR_ERR_NOMEM;
+    }
+    double sum = 0;
+    for (uint32_t i = 0; i < n; ++i) sum += w[i];
+    uint32_t ns = 0, nl = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        sc[i] = w[i] * n / sum;
+        if (sc[i] < 1.0) small[ns++] = i; else large[nl++] = i;
+    }
+    while (ns && nl) {
+        uint32_t s = small[--ns], l = large[nl - 1];
+        A->prob[s] = (float)sc[s];
+        A->alias[s] = l;
+        sc[l] = (sc[l] + sc[s]) - 1.0;
+        if (sc[l] < 1.0) { --nl; small[ns++] = l; }
+    }
+    for (uint32_t i = 0; i < nl; ++i) { A->prob[large[i]] = 1.f; A->alias[large[i]] = large[i]; }
+    for (uint32_t i = 0; i < ns; ++i) { A->prob[small[i]] = 1.f; A->alias[small[i]] = small[i]; }
+    free(sc); free(small); free(large);
+    return OR_OK;
+}
+
+static uint32_t alias_draw(const alias_t *A, uint64_t h) {
+    uint32_t col = (uint32_t)(((h >> 32) * (uint64_t)A->n) >> 32);
+    float coin = (float)(uint32_t)h * (1.0f / 4294967296.0f);
+    return coin < A->prob[col] ? col : A->alias[col];
+}
+
+int or_gen_chung_lu(uint32_t n, uint64_t m, double gamma, double wmin, double cap,
+                    uint64_t seed, or_graph *g) {
+    memset(g, 0, sizeof(*g));
+    if (n < 2 || gamma <= 1.0 || wmin <= 0) return OR_ERR_QUERY;
+    if (m > (uint64_t)n * (n - 1) / 2) return OR_ERR_QUERY;
+    const uint64_t ws = sm64(seed ^ 0x574549474854ull), es = sm64(seed ^ 0x45444745ull);
+    double *w = (double *)malloc((size_t)n * sizeof(double));
+    if (!w) return OR_ERR_NOMEM;
+    const double ex = -1.0 / (gamma - 1.0);
+    for (uint32_t i = 0; i < n; ++i) {
+        double x = wmin * pow(unit_open(sm64(ws + (uint64_t)i)), ex);
+        w[i] = x < cap ? x : cap;
+    }
+    alias_t A;
+    int rc = alias_build(w, n, &A);
+    free(w);
+    if (rc) return rc;
+    /* the first m distinct non-loop pairs of the stream t = 0, 1, 2, ...
+     * (open-addressing set of packed pairs; 0 never occurs: it is a loop) */
+    uint64_t cap_h = 1;
+    while (cap_h < 2 * m + 16) cap_h <<= 1;
+    uint64_t *set = (uint64_t *)calloc((size_t)cap_h, sizeof(uint64_t));
+    uint32_t *src = (uint32_t *)malloc((size_t)(2 * m + 1) * sizeof(uint32_t));
+    uint32_t *dst = (uint32_t *)malloc((size_t)(2 * m + 1) * sizeof(uint32_t));
+    if (!set || !src || !dst) {
+        free(set); free(src); free(dst); free(A.prob); free(A.alias);
+        return OR_ERR_NOMEM;
+    }
+    uint64_t have = 0;
+    for (uint64_t t = 0; have < m; ++t) {
+        uint32_t a = alias_draw(&A, sm64(es + 2 * t));
+        uint32_t b = alias_draw(&A, sm64(es + 2 * t + 1));
+        if (a == b) continue;
+        if (a > b) { uint32_t x = a; a = b; b = x; }
+        uint64_t key = ((uint64_t)a << 32) | b;
+        uint64_t hsh = sm64(key) & (cap_h - 1);
+        while (set[hsh] && set[hsh] != key) hsh = (hsh + 1) & (cap_h - 1);
+        if (set[hsh]) continue;
+        set[hsh] = key;
+        src[2 * have] = a; dst[2 * have] = b;
+        src[2 * have + 1] = b; dst[2 * have + 1] = a;
+        ++have;
+    }
+    free(set); free(A.prob); free(A.alias);
+    rc = or_graph_from_arcs(n, 2 * m, src, dst, g);
+    free(src); free(dst);
+    return rc;
+}
+
+int or_relabel_by_degree(const or_graph *g, or_graph *out, uint32_t *orig) {
+    memset(out, 0, sizeof(*out));
+    const uint32_t n = g->n;
+    const int sym = or_is_symmetric(g);
+    uint64_t *key = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    uint32_t *rank = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+    uint32_t *src = (uint32_t *)malloc((size_t)(g->arcs + 1) * sizeof(uint32_t));
+    uint32_t *dst = (uint32_t *)malloc((size_t)(g->arcs + 1) * sizeof(uint32_t));
+    if (!key || !rank || !src || !dst) { free(key); free(rank); free(src); free(dst); return OR_ERR_NOMEM; }
+    for (uint32_t v = 0; v < n; ++v) {
+        uint64_t d = g->out_off[v + 1] - g->out_off[v];
+        if (!sym) d += g->in_off[v + 1] - g->in_off[v];
+        key[v] = (d << 32) | v;
+    }
+    qsort(key, n, sizeof(uint64_t), cmp_u64);
+    for (uint32_t r = 0; r < n; ++r) {
+        uint32_t v = (uint32_t)(key[r] & 0xffffffffu);
+        rank[v] = r;
+        if (orig) orig[r] = v;
+    }
+    uint64_t a = 0;
+    for (uint32_t v = 0; v < n; ++v)
+        for (uint64_t i = g->out_off[v]; i < g->out_off[v + 1]; ++i) {
+            src[a] = rank[v];
+            dst[a] = rank[g->out_adj[i]];
+            ++a;
+        }
+    int rc = or_graph_from_arcs(n, a, src, dst, out);
+    free(key); free(rank); free(src); free(dst);
+    return rc;
 }

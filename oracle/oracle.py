@@ -52,6 +52,11 @@ def lib():
         L.or_count.argtypes = [gp, gp, u32p, C.c_uint32, C.c_uint32, C.c_int, u64p, u64p, u64p]
         L.or_enumerate.argtypes = [gp, gp, u32p, _CB, C.c_void_p]
         L.or_count_striped.argtypes = [gp, gp, u32p, C.c_uint32, C.c_uint32, C.c_int, u64p, u64p]
+        L.or_count_ex.argtypes = [gp, gp, u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                  C.c_int, u64p, u64p]
+        L.or_gen_chung_lu.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                      C.c_uint64, gp]
+        L.or_relabel_by_degree.argtypes = [gp, gp, u32p]
         _lib = L
     return _lib
 
@@ -95,9 +100,32 @@ class Graph:
         src = np.repeat(np.arange(n, dtype=np.uint32), deg)
         return cls.from_arrays(n, src, adj)
 
+    @classmethod
+    def chung_lu(cls, n: int, m: int, gamma: float, wmin: float, cap: float, seed: int) -> "Graph":
+        """The seeded Chung-Lu graph of the engine's generator, built here."""
+        o = cls()
+        rc = lib().or_gen_chung_lu(n, m, gamma, wmin, cap, seed, C.byref(o.g))
+        if rc:
+            raise ValueError(f"oracle generator failed ({rc})")
+        return o
+
+    def relabel_by_degree(self) -> "Tuple[Graph, np.ndarray]":
+        """(the graph with ids renamed to their (degree, id) rank, orig[rank])."""
+        o = Graph()
+        orig = np.zeros(max(self.n, 1), np.uint32)
+        rc = lib().or_relabel_by_degree(C.byref(self.g), C.byref(o.g),
+                                        orig.ctypes.data_as(C.POINTER(C.c_uint32)))
+        if rc:
+            raise ValueError(f"oracle relabel failed ({rc})")
+        return o, orig[:self.n]
+
     @property
     def n(self) -> int:
         return self.g.n
+
+    @property
+    def arcs(self) -> int:
+        return self.g.arcs
 
     def csr(self):
         n, a = self.g.n, self.g.arcs
@@ -158,6 +186,28 @@ def count_striped(d: Graph, q: Graph, shard: int, nshards: int, order_: Optional
                                 C.byref(cnt), lv)
     if rc:
         raise ValueError(f"oracle striped count failed ({rc})")
+    return cnt.value, list(lv)
+
+
+OPT_CLOSED_LAST = 1
+
+
+def count_ex(d: Graph, q: Graph, order_: Optional[Sequence[int]] = None,
+             conds: Sequence[Tuple[int, int]] = (), shard: int = 0, nshards: int = 1,
+             opts: int = 0, nthreads: int = 0):
+    """(count, level_sizes) over the roots u % nshards == shard, with
+    ordering conditions conds = [(a, b)]: the vertex matched at position a is
+    below the one at position b."""
+    k = q.n
+    cnt = C.c_uint64()
+    lv = (C.c_uint64 * k)()
+    op = (C.c_uint32 * k)(*order_) if order_ is not None else None
+    flat = [x for ab in conds for x in ab]
+    cp = (C.c_uint32 * max(len(flat), 1))(*flat)
+    rc = lib().or_count_ex(C.byref(d.g), C.byref(q.g), op, cp, len(conds), shard, nshards, opts,
+                           nthreads, C.byref(cnt), lv)
+    if rc:
+        raise ValueError(f"oracle count_ex failed ({rc})")
     return cnt.value, list(lv)
 
 
