@@ -87,6 +87,8 @@ _SIGS = {
                                 _u64p, _u64p]),
     "cuts_count_sharded": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                      _u64p, C.POINTER(C.c_float), _u64p]),
+    "cuts_count_sharded_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        _u64p, _fp, _u64p, _u64p]),
     "cuts_dump": (C.c_int, [_vp, _vp, C.c_char_p, _u64p]),
     "cuts_search": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, _u64p,
                               C.POINTER(C.c_float)]),
@@ -424,12 +426,17 @@ class Graph:
                            int(st[2]), st[3] / 1e6, st[4] / 1e6, int(st[5]), int(st[6]))
 
     def count_sharded(self, q: Query, shard: int, nshards: int, chunks: int = 1,
-                      flags: int = 0) -> CountResult:
+                      flags: int = 0, alg_bytes: bool = False, profile: bool = False) -> CountResult:
+        """The roots u with u % nshards == shard only (device ids)."""
         cnt, ms = C.c_uint64(), C.c_float()
         lv = np.zeros(q.k, np.uint64)
-        _check(lib().cuts_count_sharded(self._h, q._h, chunks, flags, shard, nshards,
-                                        C.byref(cnt), C.byref(ms), _ptr(lv, _u64p)))
-        return CountResult(cnt.value, ms.value, [int(x) for x in lv])
+        st = np.zeros(8, np.uint64)
+        st[2] = 1 if alg_bytes else 0
+        st[3] = 1 if profile else 0
+        _check(lib().cuts_count_sharded_ex(self._h, q._h, chunks, flags, shard, nshards,
+                                           C.byref(cnt), C.byref(ms), _ptr(lv, _u64p), _ptr(st, _u64p)))
+        return CountResult(cnt.value, ms.value, [int(x) for x in lv], int(st[0]), int(st[1]),
+                           int(st[2]), st[3] / 1e6, st[4] / 1e6, int(st[5]), int(st[6]))
 
     def count_budget(self, q: Query, budget_ms: float, chunks: int = 1, flags: int = 0):
         """(CountResult, finished): stops once budget_ms has passed (the host

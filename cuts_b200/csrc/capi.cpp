@@ -368,6 +368,18 @@ int cuts_count_sharded(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t fla
     return count_impl(g, q, opt, count, ms, level_sizes, nullptr);
 }
 
+int cuts_count_sharded_ex(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint32_t shard,
+                          uint32_t nshards, uint64_t *count, float *ms, uint64_t *level_sizes, uint64_t *stats) {
+    CountOptions opt;
+    opt.chunks = chunks;
+    opt.flags = flags;
+    opt.shard = shard;
+    opt.nshards = nshards;
+    opt.want_bytes = stats && stats[2] != 0;
+    opt.profile = stats && stats[3] != 0;
+    return count_impl(g, q, opt, count, ms, level_sizes, stats);
+}
+
 int cuts_count(cuts_graph g, cuts_query q, uint32_t chunks, uint32_t flags, uint64_t *count,
                float *ms) {
     return cuts_count_ex(g, q, chunks, flags, count, ms, nullptr, nullptr);

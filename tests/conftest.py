@@ -7,7 +7,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REF_DIR = "/root/reference"
+# the reference checkout: CUTS_REFERENCE_DIR, else "reference" beside the repository
+REF_DIR = os.environ.get("CUTS_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def pytest_configure(config):

@@ -108,3 +108,40 @@ def test_python_mirror(tmp_path, capfd):
     assert out.count(f"er.g,c4.g,") == 2
     with pytest.raises(cb.CutsError):
         cb.search_dfs_bfs_strategy(qpath, dpath, False, 0)
+
+
+_DUMPS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_dumps.json")
+
+
+def _dump_cases():
+    if not os.path.exists(_DUMPS):
+        return []
+    import json
+    with open(_DUMPS) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.skipif(not _dump_cases(), reason="reference dumps not recorded")
+def test_dump_sets_equal_reference_binary(tmp_path):
+    """Match sets identical to the ans.txt the reference binary wrote
+    (tests/golden/ref_dumps.json): same canonical digest, same line count."""
+    import hashlib
+    graphs = {}
+    for c in _dump_cases():
+        key = c["graph"]
+        if key not in graphs:
+            p = c["graph_params"]
+            h = (cb.HostGraph.erdos_renyi(p["n"], p["p"], p["seed"]) if c["graph_kind"] == "er" else
+                 cb.HostGraph.chung_lu(p["n"], p["m"], p["gamma"], p["wmin"], p["cap"], p["seed"]))
+            graphs[key] = h.upload(0)
+        g = graphs[key]
+        k, arcs = cb.named_query_arcs(c["query"])
+        q = cb.Query.from_arcs(k, arcs)
+        path = str(tmp_path / f"{key}_{c['query']}.txt")
+        n = g.dump(q, path)
+        rows = _parse_dump(path, q.order)
+        hsh = hashlib.sha256()
+        for r in sorted(rows):
+            hsh.update((" ".join(str(x) for x in r) + "\n").encode())
+        assert n == len(rows) == c["lines"], (key, c["query"])
+        assert hsh.hexdigest() == c["sha256"] == c["oracle_sha256"], (key, c["query"])

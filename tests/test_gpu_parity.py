@@ -401,3 +401,23 @@ def test_orbit_fold(er2k, cl5k, loops_graph, monkeypatch, name):
         monkeypatch.setenv("CUTS_FUSE_SPLIT", "0")
         assert g.count(q, flags=S).count == cnt
         monkeypatch.delenv("CUTS_FUSE_SPLIT")
+
+
+@pytest.fixture(scope="module")
+def sparse5k():
+    # mean degree 1.6 (arcs < 2n): the regime where the reference switches to
+    # its 8-lane kernel (AVG_DEGREE = arcs / n + 2 <= 3, host_funcs.cu:33,145)
+    h = cb.HostGraph.erdos_renyi(5000, 1.6 / 4999, seed=31)
+    n, arcs, sym, maxd = h.info()
+    assert arcs < 2 * n
+    return h, h.upload(0), oracle_graph_from_host(h)
+
+
+@pytest.mark.parametrize("name", ["3-path", "4-path", "5-path", "3-star", "triangle", "4-cycle"])
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK, cb.FLAG_NO_CLOSED_FORM])
+def test_sparse_graph(sparse5k, name, flags):
+    h, g, od = sparse5k
+    k, arcs = cb.named_query_arcs(name)
+    cnt = _check(g, od, k, arcs, flags=flags, chunks=3, levels=not (flags & cb.FLAG_SYMMETRY_BREAK))
+    if name.endswith("path") or name.endswith("star"):
+        assert cnt > 0
