@@ -8,48 +8,89 @@ graph with n = 1,000,000 vertices and exactly 10,000,000 distinct edges
 pendant, each counted exactly along the score.cpp order with the root level
 cut into 4 chunks, as the reference's `cuts <data> <query> 4`.  The input is
 synthetic (this project's seeded generator): the reference's SNAP graphs are
-not used.  The configuration's other two queries, house and 5-cycle, are not
-in the timed step: root-sampled level sizes put ~2.5e12 and ~4.5e13 partial
-matches at their third level (~1.4e13 and ~2.7e14 embeddings), beyond an
-exact enumeration in a benchmark run by this or any vertex-at-a-time engine.
+not used.
 
-One step = the two counts.  value = matches per second of device time
-(sum of counts / sum of device times; each count timed by CUDA events on the
-engine's stream from its first kernel to its last, as the reference times
-its search).  L2 is flushed (a 512 MB write) before every count, outside the
-timed intervals.
+One step = the two counts, with exact symmetry breaking (one embedding per
+automorphism class, scaled by |Aut|; --flags 0 enumerates every embedding).
+value = matches per second of device time (sum of counts / sum of device
+times; each count timed by CUDA events on the engine's stream from its first
+kernel to its last, as the reference times its search).  L2 is flushed (a
+512 MB write) before every count, outside the timed intervals.
+
+Beside the headline the line carries (1 GPU):
+  plain          the same two counts with no flags (every embedding enumerated);
+  all_queries    the configuration's four queries: triangle and 4-clique +
+                 pendant in full, house and 5-cycle on a root stripe (their
+                 full counts, ~1.4e13 and ~2.7e14 embeddings, take hours);
+  same_sample    the engine on exactly the root stripes the host baseline
+                 counts (counts asserted equal to the host's);
+  reference_gpu  the reference binary (built for sm_100a, resized buffers)
+                 counting the triangle with 4 trunks, run once;
+  roofline, e2e, cpu_baseline, clocks, gpu_launches.
+
+A root stripe is the roots u with u % S == 0 on degree-ranked ids (vertices
+renamed by (degree, id), ascending), so a stripe holds every S-th vertex of
+the degree order: a degree-stratified sample.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuts|reference]
 
 With N > 1 (torchrun, one rank per GPU) the roots are striped over ranks
-(u % N == rank, as the reference's multi-node level 0) and the four counts are
+(u % N == rank, as the reference's multi-node level 0) and the counts are
 summed over ranks; the total work is fixed, so scaling is "strong".
 
---impl reference times the CPU oracle (a C/OpenMP restatement of the
-reference's algorithm, the same join order) on this host's cores over a
-bounded root sample of the same workload; the reference itself has no CPU
-implementation of the search.
+--impl reference times the host oracle (a C/OpenMP restatement of the
+reference's algorithm, its own generator, relabelling and score order; the
+reference has no CPU search of its own) on every host thread over the same
+root stripes; that arm loads no part of the engine.
+
+--profile-case runs one small count sized for an ncu capture (see --help).
 """
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = {
-    "workload": "chung-lu n=1e6 m=1e7 gamma=2.1 cap=2e4 seed=0; triangle, 4-clique+pendant; chunks=4",
-    "n": 1_000_000, "m": 10_000_000, "gamma": 2.1, "wmin": 2.0, "cap": 20000.0, "seed": 0,
-    "queries": ["triangle", "4-clique+pendant"],
-    "chunks": 4,
-}
+GRAPH = dict(n=1_000_000, m=10_000_000, gamma=2.1, wmin=2.0, cap=20000.0, seed=0)
+HEADLINE = ["triangle", "4-clique+pendant"]
+CHUNKS = 4
+WORKLOAD = "chung-lu n=1e6 m=1e7 gamma=2.1 cap=2e4 seed=0; triangle, 4-clique+pendant; chunks=4"
 METRIC = "matches/s (exact counts, 1M-vertex power-law graph)"
 UNIT = "matches/s"
+# host sample: root stripe S per headline query (u % S == 0, degree ranks)
+CPU_STRIPE = {"triangle": 16, "4-clique+pendant": 2048}
+# engine-only stripes of the configuration's two other queries
+OTHER_STRIPE = {"house": 65536, "5-cycle": 65536}
+
+
+def _sym(edges):
+    return [a for e in edges for a in (e, e[::-1])]
+
+
+# the configuration's queries (undirected: both arcs per edge), defined here
+# so the host arm needs nothing from the engine package
+QUERIES = {
+    "triangle": (3, _sym([(0, 1), (1, 2), (2, 0)])),
+    "4-clique+pendant": (5, _sym([(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (0, 4)])),
+    "house": (5, _sym([(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (1, 4)])),
+    "5-cycle": (5, _sym([(i, (i + 1) % 5) for i in range(5)])),
+}
+
+
+def shared_config(n, arcs, maxd):
+    """The config object both arms print (identical by construction)."""
+    return {"workload": WORKLOAD, "n": n, "arcs": arcs, "max_degree": maxd, "queries": HEADLINE,
+            "chunks": CHUNKS,
+            "l2": "GPU counts: 512 MB write flushes L2 before every count; host counts: not applicable",
+            "host_sample": {q: f"roots u % {s} == 0 of degree-ranked ids" for q, s in CPU_STRIPE.items()}}
 
 
 def _env_rank():
@@ -120,8 +161,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+def ncu_summary():
+    """Per-launch DRAM bytes and counters of the dominant kernel from the
+    committed ncu summary (profiles/traffic.json)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         with open(p) as f:
@@ -129,112 +171,57 @@ def ncu_traffic():
     return {}
 
 
-def make_graph():
-    import cuts_b200 as cb
-    w = WORKLOAD
-    return cb.HostGraph.chung_lu(w["n"], w["m"], w["gamma"], w["wmin"], w["cap"], w["seed"])
-
-
-def make_queries():
-    import cuts_b200 as cb
-    return [(name,) + cb.named_query_arcs(name) for name in WORKLOAD["queries"]]
-
-
 # ---------------------------------------------------------------------------
-# CPU oracle (cpu_baseline and --impl reference)
+# host oracle: cpu_baseline and --impl reference
 # ---------------------------------------------------------------------------
 
-def cpu_sample(h, queries, budget_s=20.0):
-    """Time the oracle on a root sample of each query, sized so the whole sample
-    takes about budget_s seconds; returns (matches/s, cores, description)."""
+def oracle_ranked_graph():
+    """The workload graph built by the oracle's own generator, ids renamed to
+    (degree, id) ranks like the engine's device ids."""
     from oracle import oracle as O
-    import numpy as np
-    oo, oa, _, _ = h.csr()
-    od = O.Graph.from_csr(h.n, oo, oa)
-    cores = os.cpu_count() or 1
-    total_cnt, total_t, parts = 0, 0.0, []
-    per_q = budget_s / len(queries)
-    import cuts_b200 as cb
-    for name, k, arcs in queries:
-        order = cb.Query.from_arcs(k, arcs).order
+    og = O.Graph.chung_lu(GRAPH["n"], GRAPH["m"], GRAPH["gamma"], GRAPH["wmin"], GRAPH["cap"], GRAPH["seed"])
+    rg, _ = og.relabel_by_degree()
+    del og
+    return rg
+
+
+def cpu_sample(rg, cores):
+    """The oracle on the host stripe of each headline query (plain semantics,
+    its own score order, a count-only last level: the same count without one
+    step per match); returns (matches/s, per-query results, description)."""
+    from oracle import oracle as O
+    tot_c, tot_t, per, parts = 0, 0.0, {}, []
+    for name in HEADLINE:
+        S = CPU_STRIPE[name]
+        k, arcs = QUERIES[name]
         oq = O.Graph.from_arcs(k, arcs)
-        n0 = h.n
-        # grow a contiguous root slice (vertex-id order; weights are i.i.d. per
-        # vertex, so a slice is an unbiased sample) until it takes per_q / 4
-        span = 8
-        while True:
-            t0 = time.perf_counter()
-            cnt, lv, _ = O.count(od, oq, order, 0, span, cores)
-            dt = time.perf_counter() - t0
-            if dt >= per_q / 4 or span >= n0:
-                break
-            span = min(n0, span * 4 if dt < per_q / 64 else span * 2)
-        total_cnt += cnt
-        total_t += dt
-        parts.append(f"{name}: first {span} roots ({100.0 * span / n0:.3f}% of L_0) {dt:.2f}s")
-    return total_cnt / max(total_t, 1e-9), cores, "; ".join(parts)
-
-
-REF_SAFE_DEGREE = 32768 + 112   # cuts_ref_b148: per-warp helper of 32,768 words past 112 in smem
-REF_TABLE_WORDS = 3.5e9          # its trie table (u32 words, every level of a trunk)
-REF_FINAL_WORDS = 4.5e10         # its managed final table
-
-
-def reference_gpu(h, queries, level_sizes, counts, chunks):
-    """Time the reference binary (built for sm_100a, 148-SM grid, enlarged
-    candidate helper) on the workload's queries that it can run without
-    overflowing its fixed tables; the others are reported as unsafe and not
-    launched.  Returns {query: {...}}."""
-    import re
-    import tempfile
-    from oracle import oracle as O
-    binary = O.REF_CUTS.replace("cuts_ref", "cuts_ref_b148")
-    out = {}
-    if not os.path.exists(binary):
-        return {"unavailable": "oracle/_ref/cuts_ref_b148 not built"}
-    n, arcs, sym, maxd = h.info()
-    with tempfile.TemporaryDirectory() as d:
-        dpath = os.path.join(d, "data.g")
-        h.write(dpath)
-        import cuts_b200 as cb
-        for (name, k, qarcs), lv, cnt in zip(queries, level_sizes, counts):
-            stored = sum(lv[:-1])
-            final_words = cnt + (k - 1) * (lv[-2] if k >= 2 else 0)
-            if maxd >= REF_SAFE_DEGREE or stored > REF_TABLE_WORDS or final_words > REF_FINAL_WORDS:
-                out[name] = {"run": False, "reason": f"would overflow the reference's fixed tables "
-                                                     f"(levels {stored:.3g} words, final {final_words:.3g})"}
-                continue
-            qpath = os.path.join(d, name + ".g")
-            cb.write_query(qpath, k, qarcs)
-            t0 = time.perf_counter()
-            r = subprocess.run([binary, dpath, qpath, str(chunks)], capture_output=True, text=True,
-                               timeout=1800)
-            wall = time.perf_counter() - t0
-            m = None
-            for line in r.stdout.splitlines()[::-1]:
-                m = re.match(r"^(.*),(.*),([0-9.e+-]+)ms,(\d+)$", line.strip())
-                if m:
-                    break
-            if not m:
-                out[name] = {"run": True, "failed": (r.stdout + r.stderr)[-300:]}
-                continue
-            out[name] = {"run": True, "ms": float(m.group(3)), "count": int(m.group(4)),
-                         "count_matches": int(m.group(4)) == cnt, "wall_s_with_load": wall}
-    return out
+        order = O.order(oq)[0]
+        t0 = time.perf_counter()
+        cnt, lv = O.count_ex(rg, oq, order, [], 0, S, O.OPT_CLOSED_LAST, cores)
+        dt = time.perf_counter() - t0
+        tot_c += cnt
+        tot_t += dt
+        per[name] = {"stripe": S, "roots": lv[0], "count": cnt, "s": dt}
+        parts.append(f"{name}: roots u % {S} == 0 of degree ranks ({lv[0]} roots) {dt:.2f}s")
+    return tot_c / max(tot_t, 1e-9), per, "; ".join(parts)
 
 
 def run_reference(args):
+    """Host arm: the oracle port on this machine's cores; no engine code."""
     rank, world, _ = _env_rank()
     if rank != 0:
         return 0
-    h = make_graph()
-    queries = make_queries()
+    rg = oracle_ranked_graph()
+    import numpy as np
+    oo = rg.csr()[0]
+    maxd = int(np.diff(oo.astype(np.int64)).max())
+    cores = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_sample(h, queries, budget_s=args.cpu_budget / 2)
-    vals, desc, cores = [], "", 1
+        cpu_sample(rg, cores)
+    vals, desc = [], ""
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        v, cores, desc = cpu_sample(h, queries, budget_s=args.cpu_budget / 2)
+        v, per, desc = cpu_sample(rg, cores)
         vals.append(v)
     wall = time.perf_counter() - t0
     value = statistics.mean(vals)
@@ -243,11 +230,94 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded Chung-Lu generator)",
-        "config": {"workload": WORKLOAD["workload"], "sample": "root slices per query"},
+        "config": shared_config(rg.n, rg.arcs, maxd),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "counts": {q: p["count"] for q, p in per.items()},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the reference binary on the GPU (triangle; its only query here that fits
+# its fixed tables)
+# ---------------------------------------------------------------------------
+
+REF_SAFE_DEGREE = 32768 + 112   # cuts_ref_b148: per-warp helper of 32,768 words past 112 in smem
+LINE_RE = re.compile(r"^(.*),(.*),([0-9.e+-]+)ms,(\d+)$")
+
+
+def reference_gpu(h, name, want_count):
+    binary = os.path.join(ROOT, "oracle", "_ref", "cuts_ref_b148")
+    if not os.path.exists(binary):
+        return {"unavailable": "oracle/_ref/cuts_ref_b148 not built"}
+    n, arcs, sym, maxd = h.info()
+    if maxd >= REF_SAFE_DEGREE or arcs < 2 * n:
+        return {"unavailable": "input outside the reference's safe range"}
+    import cuts_b200 as cb
+    with tempfile.TemporaryDirectory() as d:
+        dpath = os.path.join(d, "data.g")
+        h.write(dpath)
+        k, qarcs = QUERIES[name]
+        qpath = os.path.join(d, name + ".g")
+        cb.write_query(qpath, k, qarcs)
+        t0 = time.perf_counter()
+        r = subprocess.run([binary, dpath, qpath, str(CHUNKS)], capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+    m = None
+    for line in r.stdout.splitlines()[::-1]:
+        m = LINE_RE.match(line.strip())
+        if m:
+            break
+    if not m:
+        return {"query": name, "failed": (r.stdout + r.stderr)[-300:]}
+    return {"query": name, "trunks": CHUNKS, "ms": float(m.group(3)), "count": int(m.group(4)),
+            "count_matches": int(m.group(4)) == want_count, "wall_s_with_text_load": wall,
+            "binary": "oracle/_ref/cuts_ref_b148 (grid 148, helper 32,768 words, dump tables 4e9+1e9)"}
+
+
+# ---------------------------------------------------------------------------
+# a small count for ncu captures
+# ---------------------------------------------------------------------------
+
+def run_profile_case(args):
+    """One seeded count sized for an ncu capture: the workload graph (or the
+    10,000-vertex ER graph with --graph c1), a small trie arena, one warm-up
+    count and --repeat counts of --query (root stripe u % --stripe == 0 when
+    --stripe > 1), or a batch of --batch seeded random queries."""
+    import cuts_b200 as cb
+    if args.graph == "c1":
+        h = cb.HostGraph.erdos_renyi(10_000, 8.0 / 9_999, 0)
+    else:
+        h = cb.HostGraph.chung_lu(GRAPH["n"], GRAPH["m"], GRAPH["gamma"], GRAPH["wmin"], GRAPH["cap"],
+                                  GRAPH["seed"])
+    g = h.upload(0)
+    g.set_arena_bytes(args.arena_mb << 20)
+    if args.batch:
+        qs = []
+        for s in range(args.batch):
+            k = 3 + s % 5
+            qs.append(cb.Query.from_arcs(k, cb.random_query_arcs(k, [0.2, 0.4, 0.6][s % 3], s)))
+        b = g.batch(qs, flags=args.flags)
+        b.run()
+        for _ in range(args.repeat):
+            counts, status, ms = b.run()
+            print(f"batch {args.batch}: {ms:.3f} ms, {sum(counts)} matches, "
+                  f"{sum(1 for s in status if s)} unfinished", flush=True)
+        return 0
+    q = cb.Query.from_arcs(*cb.named_query_arcs(args.query))
+
+    def run():
+        if args.stripe > 1:
+            return g.count_sharded(q, 0, args.stripe, chunks=CHUNKS, flags=args.flags)
+        return g.count(q, chunks=CHUNKS, flags=args.flags, stats=True)
+
+    run()
+    for _ in range(args.repeat):
+        r = run()
+        print(f"{args.query}: count {r.count} in {r.ms:.3f} ms, levels {r.level_sizes}, "
+              f"launches {r.launches}", flush=True)
     return 0
 
 
@@ -314,12 +384,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuts", choices=["cuts", "reference"])
     ap.add_argument("--flags", type=int, default=1,
-                    help="CUTS_FLAG_* bits; default 1 = symmetry breaking (exact: one embedding "
-                         "per automorphism orbit, scaled by |Aut(Q)|)")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+                    help="CUTS_FLAG_* bits of the headline step; default 1 = symmetry breaking (exact: "
+                         "one embedding per automorphism class, scaled by |Aut(Q)|)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-gpu", action="store_true",
-                    help="also time the reference binary where it is safe to run")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference binary's run")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline step, e2e and roofline only (no plain, all_queries, same_sample)")
     ap.add_argument("--workload", default="mid", choices=["mid", "learned", "batched", "large"],
                     help="mid = the headline line; the others print their own report line")
     ap.add_argument("--budget-ms", type=float, default=5000.0,
@@ -328,9 +398,20 @@ def main():
                     help="batched workload: each query's share of GPU time")
     ap.add_argument("--batch-launch-ms", type=float, default=60000.0,
                     help="batched workload: the launch's device-time budget")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one small count for an ncu capture (--query, --stripe, --repeat, --graph, "
+                         "--arena-mb, --batch; --flags applies)")
+    ap.add_argument("--query", default="triangle")
+    ap.add_argument("--stripe", type=int, default=1)
+    ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--graph", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--arena-mb", type=int, default=1024)
+    ap.add_argument("--batch", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_case:
+        return run_profile_case(args)
     if args.workload != "mid":
         return run_other_workload(args)
 
@@ -348,24 +429,23 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    h = make_graph()
+    h = cb.HostGraph.chung_lu(GRAPH["n"], GRAPH["m"], GRAPH["gamma"], GRAPH["wmin"], GRAPH["cap"], GRAPH["seed"])
     n, arcs, sym, maxd = h.info()
     g = h.upload(dev)
-    queries = [(name, cb.Query.from_arcs(k, a)) for name, k, a in make_queries()]
-    chunks = WORKLOAD["chunks"]
+    queries = [(name, cb.Query.from_arcs(*QUERIES[name])) for name in HEADLINE]
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
 
-    def count(q):
+    def count(q, flags, stats=True):
         if world > 1:
-            return g.count_sharded(q, rank, world, chunks=chunks, flags=args.flags)
-        return g.count(q, chunks=chunks, flags=args.flags, stats=True)
+            return g.count_sharded(q, rank, world, chunks=CHUNKS, flags=flags)
+        return g.count(q, chunks=CHUNKS, flags=flags, stats=stats)
 
-    def step(record):
+    def step(record, flags):
         ms, cnts, launches = 0.0, [], 0
         for name, q in queries:
             flush.fill_(len(cnts))
             torch.cuda.synchronize(dev)
-            r = count(q)
+            r = count(q, flags)
             ms += r.ms
             cnts.append(r.count)
             launches += r.launches
@@ -374,7 +454,7 @@ def main():
         return ms, cnts, launches
 
     for _ in range(args.warmup):
-        step(None)
+        step(None, args.flags)
 
     clocks = Clocks(dev)
     if pg:
@@ -385,7 +465,7 @@ def main():
     total_ms, launches, per_query = 0.0, 0, []
     counts = None
     for _ in range(args.steps):
-        ms, cnts, la = step(per_query)
+        ms, cnts, la = step(per_query, args.flags)
         total_ms += ms
         launches += la
         counts = cnts
@@ -419,9 +499,9 @@ def main():
         cnt_e = []
         for name, q in queries:
             if world > 1:
-                cnt_e.append(g2.count_sharded(q, rank, world, chunks=chunks, flags=args.flags).count)
+                cnt_e.append(g2.count_sharded(q, rank, world, chunks=CHUNKS, flags=args.flags).count)
             else:
-                cnt_e.append(g2.count(q, chunks=chunks, flags=args.flags).count)
+                cnt_e.append(g2.count(q, chunks=CHUNKS, flags=args.flags).count)
         g2.close()
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t1
@@ -436,66 +516,111 @@ def main():
 
     result = None
     if rank == 0:
-        # live per-kernel timing for the roofline: one profiled pass (event
-        # pairs around every level launch) plus the traffic model
-        kern = {"last_level": [0.0, 0, 0], "expand": [0.0, 0, 0]}
+        peak, peak_kind = measured_peaks()
+        ncu = ncu_summary()
+        roofline = {"kernel": None, "bound": "l2", "achieved": None, "peak": peak, "unit": "GB/s",
+                    "frac": None, "traffic": ncu.get("last_level_bytes_per_launch"), "peak_source": peak_kind}
+        extras = {}
         if world == 1:
+            # live per-kernel timing for the roofline: one profiled pass (event
+            # pairs around every level launch) plus the traffic model
+            ll_ms, ll_n, ll_bytes, ex_ms = 0.0, 0, 0, 0.0
+            kinds = []
             for name, q in queries:
                 flush.fill_(7)
                 torch.cuda.synchronize(dev)
-                r = g.count(q, chunks=chunks, flags=args.flags, stats=True, profile=True,
-                            alg_bytes=True)
-                kern["last_level"][0] += r.last_level_ms
-                kern["last_level"][1] += r.last_level_launches
-                kern["last_level"][2] += r.last_level_bytes
-                kern["expand"][0] += r.expand_ms
-                kern["expand"][1] += r.expand_launches
-        peak, peak_kind = measured_peaks()
-        ll_ms, ll_n, ll_bytes = kern["last_level"]
-        achieved = (ll_bytes / max(ll_n, 1)) / ((ll_ms / max(ll_n, 1)) / 1e3) / 1e9 if ll_ms else None
-        traffic = ncu_traffic().get("last_level_bytes_per_launch")
-        # the counting kernel of each query: fused with the level before, or flat
-        sym = h.info()[2]
-        kinds = []
-        for name, q in queries:
-            lv, _ = q.plan_levels(sym, args.flags)
-            fused = any(x["fuse"] for x in lv) and os.environ.get("CUTS_NO_FUSE") != "1"
-            kinds.append(f"{'k_fused' if fused else 'k_level_flat'}<count> ({name})")
-        roofline = {
-            "kernel": "last counted level: " + ", ".join(kinds),
-            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-            "peak_source": peak_kind,
-            "alg_bytes_per_launch": ll_bytes / max(ll_n, 1) if ll_n else None,
-            "avg_launch_ms": ll_ms / max(ll_n, 1) if ll_n else None,
-            "share_of_kernel_time": ll_ms / max(ll_ms + kern["expand"][0], 1e-12) if ll_ms else None,
-        }
-
+                r = g.count(q, chunks=CHUNKS, flags=args.flags, stats=True, profile=True, alg_bytes=True)
+                ll_ms += r.last_level_ms
+                ll_n += r.last_level_launches
+                ll_bytes += r.last_level_bytes
+                ex_ms += r.expand_ms
+                lv, _ = q.plan_levels(sym, args.flags)
+                fused = any(x["fuse"] for x in lv) and os.environ.get("CUTS_NO_FUSE") != "1"
+                kinds.append(f"{'k_fused' if fused else 'k_level_flat'}<count> ({name})")
+            achieved = (ll_bytes / max(ll_n, 1)) / ((ll_ms / max(ll_n, 1)) / 1e3) / 1e9 if ll_ms else None
+            roofline.update({
+                "kernel": "last counted level: " + ", ".join(kinds),
+                "achieved": achieved, "frac": (achieved / peak) if achieved else None,
+                "alg_bytes_per_launch": ll_bytes / max(ll_n, 1) if ll_n else None,
+                "avg_launch_ms": ll_ms / max(ll_n, 1) if ll_n else None,
+                "share_of_kernel_time": ll_ms / max(ll_ms + ex_ms, 1e-12) if ll_ms else None,
+                "dram_frac_ncu": ncu.get("dram_throughput_frac"),
+                "l2_hit_rate_ncu": ncu.get("l2_hit_rate"),
+                "l2_throughput_frac_ncu": ncu.get("l2_throughput_frac"),
+                "note": "achieved = algorithmic bytes (every list read and probe the algorithm makes) per "
+                        "launch / CUDA-event time; the 90 MB graph is served from L2, so the kernel is "
+                        "bound by L2 latency and issue (dram_frac_ncu), and frac is against HBM copy "
+                        "bandwidth as the measurement asks",
+            })
 
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            v, cores, desc = cpu_sample(h, [(nm,) + cb.named_query_arcs(nm) for nm, _ in queries],
-                                        budget_s=args.cpu_budget)
+            rg = oracle_ranked_graph()
+            cores = os.cpu_count() or 1
+            v, per, desc = cpu_sample(rg, cores)
+            del rg
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+            # the engine on exactly the host's stripes, both flag settings
+            same = {}
+            for name, q in queries:
+                S = CPU_STRIPE[name]
+                row = {"stripe": S, "host_count": per[name]["count"], "host_s": per[name]["s"]}
+                for fl in (0, args.flags):
+                    flush.fill_(3)
+                    torch.cuda.synchronize(dev)
+                    r = g.count_sharded(q, 0, S, chunks=CHUNKS, flags=fl)
+                    row[f"flags{fl}"] = {"count": r.count, "ms": r.ms}
+                assert row["flags0"]["count"] == per[name]["count"], (name, row)
+                row["counts_equal"] = True
+                row["speedup_plain_vs_host"] = per[name]["s"] * 1e3 / max(row["flags0"]["ms"], 1e-9)
+                same[name] = row
+            extras["same_sample"] = same
+
+        if world == 1 and not args.no_extras:
+            # plain: every embedding enumerated, the same two full counts
+            plain = {}
+            for name, q in queries:
+                flush.fill_(5)
+                torch.cuda.synchronize(dev)
+                r = g.count(q, chunks=CHUNKS, flags=0, stats=True)
+                plain[name] = {"count": r.count, "ms": r.ms, "launches": r.launches}
+                assert r.count == counts[HEADLINE.index(name)]
+            tot_ms = sum(p["ms"] for p in plain.values())
+            extras["plain"] = {"flags": 0, "queries": plain, "ms_per_step": tot_ms,
+                               "value": step_matches / (tot_ms / 1e3), "unit": UNIT}
+            # all four queries of the configuration
+            allq = {}
+            for name in ["triangle", "4-clique+pendant"]:
+                allq[name] = {"stripe": 1, "flags0": plain[name],
+                              f"flags{args.flags}": {"count": counts[HEADLINE.index(name)],
+                                                     "ms": statistics.mean([t for a, c, t in per_query
+                                                                            if a == name])}}
+            for name, S in OTHER_STRIPE.items():
+                q = cb.Query.from_arcs(*QUERIES[name])
+                row = {"stripe": S, "roots": f"u % {S} == 0 of degree ranks"}
+                for fl in (0, args.flags):
+                    flush.fill_(9)
+                    torch.cuda.synchronize(dev)
+                    r = g.count_sharded(q, 0, S, chunks=CHUNKS, flags=fl)
+                    row[f"flags{fl}"] = {"count": r.count, "ms": r.ms, "levels": r.level_sizes}
+                assert row["flags0"]["count"] == row[f"flags{args.flags}"]["count"]
+                allq[name] = row
+            extras["all_queries"] = allq
 
         ref_gpu = None
-        if args.ref_gpu and world == 1:
-            lvls = []
-            for name, q in queries:
-                lvls.append(g.count(q, chunks=chunks, stats=True).level_sizes)
-            ref_gpu = reference_gpu(h, make_queries(), lvls, counts, chunks)
+        if world == 1 and not args.no_ref_gpu:
+            ref_gpu = reference_gpu(h, "triangle", counts[HEADLINE.index("triangle")])
 
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded Chung-Lu generator; SNAP graphs not used)",
-            "config": {"workload": WORKLOAD["workload"], "n": n, "arcs": arcs, "max_degree": maxd,
-                       "flags": args.flags, "l2": "flushed (512 MB write) before every count",
-                       "parallelism": f"root stripes x{world}" if world > 1 else "1 GPU"},
-            "counts": dict(zip([nm for nm, _ in queries], counts)),
+            "config": shared_config(n, arcs, maxd),
+            "method": {"flags": args.flags, "parallelism": f"root stripes x{world}" if world > 1 else "1 GPU"},
+            "counts": dict(zip(HEADLINE, counts)),
             "ms_per_query": {nm: statistics.mean([t for a, c, t in per_query if a == nm])
-                             for nm, _ in queries} if world == 1 else None,
+                             for nm in HEADLINE} if world == 1 else None,
             "wall_s_timed": wall,
             "clocks": clk,
             "gpu_launches": launches,
@@ -507,6 +632,7 @@ def main():
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
         }
+        result.update(extras)
         print(json.dumps(result), flush=True)
     if pg:
         pg.barrier()
