@@ -71,6 +71,7 @@ _SIGS = {
     "cuts_graph_from_csr": (C.c_int, [C.c_uint32, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]),
     "cuts_graph_info": (C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_int), _u32p]),
     "cuts_graph_set_level_cap": (C.c_int, [_vp, C.c_uint64]),
+    "cuts_graph_set_fuse_split": (C.c_int, [_vp, C.c_uint32]),
     "cuts_graph_set_arena_bytes": (C.c_int, [_vp, C.c_uint64]),
     "cuts_graph_free": (None, [_vp]),
     "cuts_query_load": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
@@ -408,6 +409,10 @@ class Graph:
 
     def set_arena_bytes(self, nbytes: int) -> None:
         _check(lib().cuts_graph_set_arena_bytes(self._h, nbytes))
+
+    def set_fuse_split(self, split: int) -> None:
+        """|S| above which the fused count splits a parent over all warps (0 = default)."""
+        _check(lib().cuts_graph_set_fuse_split(self._h, split))
 
     def count(self, q: Query, chunks: int = 1, flags: int = 0, stats: bool = False,
               alg_bytes: bool = False, profile: bool = False) -> CountResult:

@@ -1,10 +1,18 @@
-"""Autotuner for the batched engine's launch shape.
+"""Autotuners for the engine's work sizes.
 
-Tries each (grain, tasks per grab, blocks per SM) on a sample of the batch,
-replays each candidate's captured CUDA graph a few times, and keeps the
-fastest configuration whose counts agree with the first one tried (the count
-never depends on the shape; disagreement would be a bug and raises).
-Results can be stored per GPU model and graph in a small JSON file.
+tune_batch: the batched engine's launch shape -- (grain: level-1 candidates
+per task, i.e. the work-stealing grain; tasks per work-counter grab; blocks
+per SM) on a sample of the batch, replaying each candidate's captured CUDA
+graph a few times.
+
+tune_count: the level engine's chunk and tile sizes for one query -- the
+number of root slices (the reference's trunks), the level capacity that
+cuts the stored levels into memory chunks, and the fused count's tile (the
+candidate-set size above which a parent is split over all warps).
+
+Both keep the fastest configuration whose counts agree with the first one
+tried (a count never depends on these sizes; disagreement would be a bug and
+raises).  Results can be stored per GPU model and graph in a small JSON file.
 """
 from __future__ import annotations
 
@@ -16,6 +24,9 @@ from typing import Dict, Iterable, List, Optional, Sequence, Tuple
 import cuts_b200 as cb
 
 GRAINS = (16, 32, 64, 128, 256)
+CHUNKS = (1, 2, 4, 8)
+SPLITS = (64, 128, 256)
+LEVEL_CAPS = (0,)
 GRABS = (1, 4)
 BLOCKS = (0, 4)
 
@@ -57,6 +68,40 @@ def tune_batch(g: "cb.Graph", queries: Sequence["cb.Query"], flags: int = 0,
     if not times:
         return (64, 1, 0), times
     best = min(times, key=times.get)
+    return best, times
+
+
+def tune_count(g: "cb.Graph", q: "cb.Query", flags: int = 0, chunks: Iterable[int] = CHUNKS,
+               splits: Iterable[int] = SPLITS, level_caps: Iterable[int] = LEVEL_CAPS, reps: int = 3,
+               apply: bool = True):
+    """Returns (best (chunks, split, level cap), {config: median device ms}).
+    With apply, the graph keeps the best split and level cap afterwards
+    (chunks is an argument of each count); otherwise both return to their
+    defaults."""
+    times: Dict[Tuple[int, int, int], float] = {}
+    ref: Optional[int] = None
+    try:
+        for ch in chunks:
+            for sp in splits:
+                for cap in level_caps:
+                    g.set_fuse_split(sp)
+                    g.set_level_cap(cap)
+                    ms = []
+                    for _ in range(reps):
+                        r = g.count(q, chunks=ch, flags=flags)
+                        if ref is None:
+                            ref = r.count
+                        elif r.count != ref:
+                            raise RuntimeError(f"count depends on the work sizes {ch, sp, cap}")
+                        ms.append(r.ms)
+                    times[(ch, sp, cap)] = statistics.median(ms)
+    finally:
+        g.set_fuse_split(0)
+        g.set_level_cap(0)
+    best = min(times, key=times.get)
+    if apply:
+        g.set_fuse_split(best[1])
+        g.set_level_cap(best[2])
     return best, times
 
 

@@ -524,7 +524,7 @@ int Batch::capture(unsigned long long budget_ns) {
     cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * 2, s);
     if (nb) {
         k_batch<<<blocks, kBW * 32, 0, s>>>(
-            DevView{g->out_info, g->in_info, g->adj, g->n}, d_queries, nb, d_qbase, g->batch_vsorted,
+            graph_view(*g), d_queries, nb, d_qbase, g->batch_vsorted,
             pref, g->symmetric ? pref : pref + stride, g->symmetric ? pref : pref + 2 * stride, tune.grain,
             tune.tasks_per_grab, d_ctr, reinterpret_cast<uint32_t *>(d_ctr + 1), d_counts, d_aborted,
             budget_ns, d_qtime, qlimit, shard, nshards);
@@ -778,7 +778,7 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
             return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: plan upload failed");
     }
     const DevView view{reinterpret_cast<const uint2 *>(info_out),
-                       reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n};
+                       reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n, nullptr, nullptr};
     const unsigned long long total = (unsigned long long)nq * n;
     const uint32_t grid = uint32_t(std::min<unsigned long long>(blocks, (total + kBW - 1) / kBW));
     k_batch_noalloc<<<std::max<uint32_t>(grid, 1), kBW * 32, 0, stream>>>(view, sc, nq, counts);

@@ -207,6 +207,12 @@ int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries) {
     return CUTS_OK;
 }
 
+int cuts_graph_set_fuse_split(cuts_graph g, uint32_t split) {
+    if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
+    g->dev->fuse_split = split;
+    return CUTS_OK;
+}
+
 int cuts_graph_set_arena_bytes(cuts_graph g, uint64_t bytes) {
     if (!g || !g->dev) return set_error(CUTS_ERR_ARG, "null graph");
     DeviceGraph &d = *g->dev;

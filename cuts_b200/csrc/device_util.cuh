@@ -14,8 +14,17 @@ struct DevView {
     const uint2 *in_info;
     const uint32_t *adj;
     uint32_t n;
+    // per vertex: entries of its out- (in-) list below the vertex itself
+    // (may be null: the lists are searched instead)
+    const uint32_t *bwd_out;
+    const uint32_t *bwd_in;
 };
 
+// The kernels' view of a resident graph (a DeviceGraph).
+template <class G>
+inline DevView graph_view(const G &g) {
+    return DevView{g.out_info, g.in_info, g.adj, g.n, g.bwd_out, g.bwd_in};
+}
 
 __device__ __forceinline__ uint32_t lbound(const uint32_t *__restrict__ a, uint32_t len,
                                            uint32_t x) {
@@ -51,6 +60,23 @@ __device__ __forceinline__ uint32_t lbound_from(const uint32_t *__restrict__ a, 
         else n = half;
     }
     return lo;
+}
+
+// Lower bound of x in the list of vertex u (direction in_dir), where the
+// list's window often starts or ends at u itself (x == u + 1 or x == u, the
+// ordering conditions of symmetry breaking on degree-ranked ids): those two
+// are read from the per-vertex count of entries below u instead of searched.
+// `loops`: the graph has self-loops, so u may list itself.
+__device__ __forceinline__ uint32_t lbound_own(const DevView &g, bool in_dir, uint32_t u,
+                                               const uint32_t *__restrict__ list, uint32_t len, uint32_t x,
+                                               bool loops) {
+    const uint32_t *bw = in_dir ? g.bwd_in : g.bwd_out;
+    if (bw && (x == u || x == u + 1)) {
+        uint32_t b = __ldg(bw + u);
+        if (x == u + 1 && loops && b < len && __ldg(list + b) == u) ++b;
+        return b;
+    }
+    return lbound(list, len, x);
 }
 
 __device__ __forceinline__ uint32_t warp_min(uint32_t v) {

@@ -500,8 +500,10 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
             for (uint32_t msk = sL.gt_mask; msk; msk &= msk - 1) lo = max(lo, sm_m[warp][__ffs(msk) - 1][lane] + 1);
             for (uint32_t msk = sL.lt_mask; msk; msk &= msk - 1) hi = min(hi, sm_m[warp][__ffs(msk) - 1][lane]);
             const uint32_t *lst = g.adj + moff;
-            s0 = lo ? lbound(lst, mdeg, lo) : 0;
-            e0 = hi != kFullMask ? lbound(lst, mdeg, hi) : mdeg;
+            const uint32_t mu = nj ? sm_m[warp][sL.jpos[tmin]][lane] : 0;
+            const bool mdir = nj && sL.jdir[tmin];
+            s0 = lo ? lbound_own(g, mdir, mu, lst, mdeg, lo, loops) : 0;
+            e0 = hi != kFullMask ? lbound_own(g, mdir, mu, lst, mdeg, hi, loops) : mdeg;
             if (e0 < s0) e0 = s0;
             if (need_ub)
                 for (uint32_t t = 0; t < sN.nj; ++t)
@@ -702,20 +704,32 @@ struct FusedBig {
     unsigned long long pool_words;
 };
 
-// 12 resident blocks (48 warps) per SM: the kernel waits on dependent L2
-// loads, and the extra warps outweigh the spills the 40-register cap costs
+// Phase 1 keeps a parent's candidate set S in shared memory when it holds at
+// most kTS vertices; every pair (s, t) of S is then tested by a lane-balanced
+// walk (see pair_walk below).
+constexpr uint32_t kTS = 256;
+constexpr uint32_t kHS = 512;  // hash slots of the admissible t, buckets of 4 (load at most 1/2)
+
+// 8 resident blocks (32 warps) per SM at up to 64 registers: the pair walk
+// keeps its row state in registers
 template <int MODE>
-__global__ void __launch_bounds__(kZW * 32, 12)
+__global__ void __launch_bounds__(kZW * 32, 8)
 k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb, uint32_t phase,
         uint32_t split, uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride, FusedBig big,
         unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,
-        unsigned long long *__restrict__ acc_p) {
+        unsigned long long *__restrict__ acc_p, uint32_t walk_ok) {
     __shared__ LevelPlan sP, sC, sF;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
     __shared__ uint32_t wm[kZW][kMaxK];
     __shared__ uint32_t joff[kZW][kMaxJ], jdeg[kZW][kMaxJ];
     __shared__ uint32_t xoff[kZW][kMaxJ], xdeg[kZW][kMaxJ];
+    // the pair walk's per-parent tables: S, and a hash table of the vertices
+    // admissible as t (keys in buckets of 4, their index in S and term B)
+    __shared__ uint32_t tS[MODE == kCountMode ? kZW : 1][kTS];
+    __shared__ uint4 tHK[MODE == kCountMode ? kZW : 1][kHS / 4];
+    __shared__ uint8_t tHI[MODE == kCountMode ? kZW : 1][kHS];
+    __shared__ int32_t tHB[MODE == kCountMode ? kZW : 1][kHS];
     {
         const uint32_t words = sizeof(LevelPlan) / 4;
         const uint32_t c = p + 1;
@@ -785,8 +799,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 const uint32_t ts = lo_t ? lbound(S, ns, lo_t) : 0;
                 const uint32_t te = hi_t != kFullMask ? lbound(S, ns, hi_t) : ns;
                 const uint32_t *Ls = g.adj + lsoff;
-                const uint32_t ls0 = lo_t ? lbound(Ls, ds, lo_t) : 0;
-                const uint32_t ls1 = hi_t != kFullMask ? lbound(Ls, ds, hi_t) : ds;
+                const bool sdir = sC.jdir[tp] != 0;
+                const uint32_t ls0 = lo_t ? lbound_own(g, sdir, sv, Ls, ds, lo_t, loops) : 0;
+                const uint32_t ls1 = hi_t != kFullMask ? lbound_own(g, sdir, sv, Ls, ds, hi_t, loops) : ds;
                 const uint32_t nS = te > ts ? te - ts : 0, nL = ls1 > ls0 ? ls1 - ls0 : 0;
                 iters = nS <= nL ? 1u : 0u;  // iterate the shorter side
                 nit = iters ? nS : nL;
@@ -1006,6 +1021,245 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
         __syncwarp();
     };
 
+    // Level c over all pairs of a parent whose S fits tS (phase 1).  A pair
+    // (s, t) of S counts when t lies in s's list, inside s's window (t > s
+    // or t < s when the plan orders them; t != s otherwise), and passes the
+    // tests that depend on t alone (window of the positions below p, the
+    // extra lists, the signature); its weight splits as A(s) + B(t):
+    //   no fold:     1 + 0;
+    //   orbit fold:  (orbit base with s at p) - #orbit positions below c,
+    //                plus, when c is in the orbit, |L(t)| - c - [t loops];
+    //   plain fold:  f_base(s) - [t in the fold's window and list], the fold's
+    //                list and window fixed by the positions below p
+    //                (walk_ok is set only then).
+    // The admissible t go into a hash table in shared memory (buckets of
+    // four keys read with one 128-bit load; each slot keeps B(t) and t's
+    // index in S).  Each s's list window is then streamed with 128-bit
+    // loads: the windows of 32 vertices s (one per lane, each lane also
+    // holding its A(s)) form one sequence of 16-byte quads spread over the
+    // lanes, two quads per lane per step (owner found by a binary search
+    // over the lanes' inclusive scan), and each of the four list entries of
+    // a quad is looked up in the table -- coalesced global reads and
+    // shared-memory probes instead of a search in a list and a gather of
+    // the pendant's weight per pair.
+    auto pair_walk = [&](uint32_t ns, uint32_t lo_c, uint32_t hi_c) {
+        uint32_t *const S = tS[warp];
+        const long long akc = (cfold && sF.ofold) ? __popc(sF.ofold & ((1u << c) - 1)) : 0;
+        const bool c_in_orbit = cfold && sF.ofold && ((sF.ofold >> c) & 1u);
+        const bool p_in_orbit = cfold && sF.ofold && ((sF.ofold >> p) & 1u);
+        // plain fold: the fold's list and window, fixed for this parent
+        uint32_t f_off = 0, f_deg = 0, f_lo = 0, f_hi = kFullMask, f_ws = 0, f_we = 0, f_sub = 0;
+        if (cfold && !sF.ofold) {
+            const uint32_t u = my_m[sF.jpos[0]];
+            const uint2 inf = sF.jdir[0] ? g.in_info[u] : g.out_info[u];
+            f_off = inf.x;
+            f_deg = inf.y;
+            for (uint32_t msk = sF.gt_mask & below; msk; msk &= msk - 1) f_lo = max(f_lo, my_m[__ffs(msk) - 1] + 1);
+            for (uint32_t msk = sF.lt_mask & below; msk; msk &= msk - 1) f_hi = min(f_hi, my_m[__ffs(msk) - 1]);
+            const uint32_t *fl = g.adj + f_off;
+            f_ws = f_lo ? lbound(fl, f_deg, f_lo) : 0;
+            f_we = f_hi != kFullMask ? lbound(fl, f_deg, f_hi) : f_deg;
+            for (uint32_t j = 0; j < p; ++j) {
+                const uint32_t mj = my_m[j];
+                if (mj >= f_lo && mj < f_hi && (((sF.guar_mask >> j) & 1u) || contains(fl, f_deg, mj))) ++f_sub;
+            }
+        }
+        // orbit fold: the part of the orbit base fixed by the positions below
+        // p (the lists of the orbit positions x < p, minus the members the
+        // positions below p put there)
+        uint32_t ob_par = 0;
+        const uint32_t ob_low = (cfold && sF.ofold) ? (sF.ofold & below) : 0;
+        for (uint32_t xm = ob_low; xm; xm &= xm - 1) {
+            const uint32_t x = __ffs(xm) - 1;
+            const uint2 inf = sF.jdir[0] ? g.in_info[my_m[x]] : g.out_info[my_m[x]];
+            uint32_t sub = 0;
+            for (uint32_t j = 0; j < p; ++j)
+                if (((sF.oguar[x] >> j) & 1u) || contains(g.adj + inf.x, inf.y, my_m[j])) ++sub;
+            ob_par += inf.y - sub;
+        }
+        // the table: buckets of 4 slots (one 128-bit shared load), a power of
+        // two of at least one bucket per two vertices of S, 8..kHS/4; a full
+        // bucket continues in the next one
+        uint32_t lg = 3;
+        while ((1u << lg) * 2 < ns && (1u << lg) < kHS / 4) ++lg;
+        const uint32_t bmask = (1u << lg) - 1;
+        const uint32_t hshift = 32 - lg;
+        uint4 *const HK4 = tHK[warp];
+        uint32_t *const HK = reinterpret_cast<uint32_t *>(tHK[warp]);
+        uint8_t *const HI = tHI[warp];
+        int32_t *const HB = tHB[warp];
+        const bool need_idx = !c_gt_s && !c_lt_s && loops;
+        for (uint32_t x = lane; x <= bmask; x += 32) HK4[x] = make_uint4(kFullMask, kFullMask, kFullMask, kFullMask);
+        __syncwarp();
+        // the admissible t, with B(t), into the table
+        uint32_t nv = 0;
+        for (uint32_t i0 = 0; i0 < ns; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            bool ok = i < ns;
+            const uint32_t v = ok ? S[i] : 0;
+            if (ok) {
+                ok = v >= lo_c && v < hi_c;
+                if (ok && extra)
+                    for (uint32_t tt = 0; tt < sC.nj; ++tt)
+                        if ((extra >> tt) & 1u)
+                            if (!contains(g.adj + xoff[warp][tt], xdeg[warp][tt], v)) { ok = false; break; }
+                if (ok && sig_c) {
+                    const uint2 o = g.out_info[v], i2 = g.in_info[v];
+                    ok = i2.y >= sC.qin && o.y >= sC.qout;
+                }
+            }
+            if (ok) {
+                int32_t b = 0;
+                if (c_in_orbit) {
+                    const uint2 vi = sF.jdir[0] ? g.in_info[v] : g.out_info[v];
+                    b = int32_t(vi.y) - int32_t(c) - ((loops && contains(g.adj + vi.x, vi.y, v)) ? 1 : 0);
+                } else if (cfold && !sF.ofold) {
+                    const bool h = v >= f_lo && v < f_hi && (fguar_t || contains(g.adj + f_off, f_deg, v));
+                    b = h ? -1 : 0;
+                }
+                uint32_t bk = (v * 2654435769u) >> hshift;
+                while (true) {
+                    uint32_t slot = kFullMask;
+                    #pragma unroll
+                    for (uint32_t q = 0; q < 4; ++q)
+                        if (slot == kFullMask && atomicCAS(&HK[bk * 4 + q], kFullMask, v) == kFullMask) slot = bk * 4 + q;
+                    if (slot != kFullMask) {
+                        HI[slot] = uint8_t(i);
+                        HB[slot] = b;
+                        break;
+                    }
+                    bk = (bk + 1) & bmask;
+                }
+            }
+            nv += __popc(__ballot_sync(kFullMask, ok));
+        }
+        if (nv == 0) return;
+        __syncwarp();
+        long long sum = 0;
+        unsigned long long hits = 0;
+        const uint4 *const adj4 = reinterpret_cast<const uint4 *>(g.adj);
+        for (uint32_t r0 = 0; r0 < ns; r0 += 32) {
+            // this lane's row: s = S[r0 + lane], its list window as quads and
+            // its term A(s)
+            const uint32_t i = r0 + lane;
+            uint32_t ea = 0, eb = 0, nq = 0, arow = 1;
+            if (i < ns) {
+                const uint32_t sv = S[i];
+                const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
+                const uint32_t *Ls = g.adj + is.x;
+                uint32_t lo_v = lo_c, hi_v = hi_c;
+                if (c_gt_s) lo_v = max(lo_v, sv + 1);
+                if (c_lt_s) hi_v = min(hi_v, sv);
+                const bool sdir = sC.jdir[tp] != 0;
+                const uint32_t p0 = lo_v ? lbound_own(g, sdir, sv, Ls, is.y, lo_v, loops) : 0;
+                const uint32_t p1 = hi_v != kFullMask ? lbound_own(g, sdir, sv, Ls, is.y, hi_v, loops) : is.y;
+                if (p1 > p0) {
+                    ea = is.x + p0;
+                    eb = is.x + p1;
+                    nq = ((eb + 3) >> 2) - (ea >> 2);
+                    // A(s): the orbit base with s at p (orbit_base's sum, the
+                    // parent's part computed once), or the plain fold's base
+                    if (cfold && sF.ofold) {
+                        arow = ob_par;
+                        for (uint32_t xm = ob_low; xm; xm &= xm - 1) {
+                            const uint32_t x = __ffs(xm) - 1;
+                            if ((sF.oguar[x] >> p) & 1u) {
+                                --arow;
+                            } else {
+                                const uint2 xi = sF.jdir[0] ? g.in_info[my_m[x]] : g.out_info[my_m[x]];
+                                if (contains(g.adj + xi.x, xi.y, sv)) --arow;
+                            }
+                        }
+                        if (p_in_orbit) {
+                            const uint2 vi = sF.jdir[0] ? g.in_info[sv] : g.out_info[sv];
+                            uint32_t sub = (((sF.oguar[p] >> p) & 1u) || (loops && contains(g.adj + vi.x, vi.y, sv)))
+                                               ? 1u : 0u;
+                            for (uint32_t j = 0; j < p; ++j)
+                                if (((sF.oguar[p] >> j) & 1u) || contains(g.adj + vi.x, vi.y, my_m[j])) ++sub;
+                            arow += vi.y - sub;
+                        }
+                    } else if (cfold) {
+                        const bool in = sv >= f_lo && sv < f_hi &&
+                                        (((sF.guar_mask >> p) & 1u) || contains(g.adj + f_off, f_deg, sv));
+                        arow = (f_we > f_ws ? f_we - f_ws : 0) - f_sub - (in ? 1u : 0u);
+                    }
+                }
+            }
+            uint32_t incl = nq;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t qtotal = __shfl_sync(kFullMask, incl, 31);
+            const uint32_t excl = incl - nq;
+            // two quads per lane per step (more loads in flight)
+            for (uint32_t fstep = 0; fstep < qtotal; fstep += 64) {
+                uint32_t quad[2], qea[2], qeb[2], qoi[2], qa[2];
+                bool have[2];
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t f = fstep + 32 * h + lane;
+                    uint32_t owner = 0;
+                    #pragma unroll
+                    for (int step = 16; step; step >>= 1) {
+                        const uint32_t probe = __shfl_sync(kFullMask, incl, int(owner + step - 1));
+                        if (probe <= f) owner += step;
+                    }
+                    owner = min(owner, 31u);
+                    const int ow = int(owner);
+                    const uint32_t o_excl = __shfl_sync(kFullMask, excl, ow);
+                    qea[h] = __shfl_sync(kFullMask, ea, ow);
+                    qeb[h] = __shfl_sync(kFullMask, eb, ow);
+                    qa[h] = __shfl_sync(kFullMask, arow, ow);
+                    have[h] = f < qtotal;
+                    qoi[h] = r0 + owner;
+                    quad[h] = (qea[h] >> 2) + (f - o_excl);
+                }
+                uint4 xq[2];
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) xq[h] = have[h] ? __ldg(adj4 + quad[h]) : make_uint4(0, 0, 0, 0);
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (!have[h]) continue;
+                    const uint32_t e0 = quad[h] << 2;
+                    const uint32_t vals[4] = {xq[h].x, xq[h].y, xq[h].z, xq[h].w};
+                    uint32_t cnt = 0;
+                    long long bs = 0;
+                    #pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t e = e0 + uint32_t(k);
+                        if (e < qea[h] || e >= qeb[h]) continue;
+                        const uint32_t v = vals[k];
+                        uint32_t bk = (v * 2654435769u) >> hshift;
+                        while (true) {
+                            const uint4 kk = HK4[bk];
+                            const uint32_t eq = (kk.x == v ? 1u : 0u) | (kk.y == v ? 2u : 0u) |
+                                                (kk.z == v ? 4u : 0u) | (kk.w == v ? 8u : 0u);
+                            if (eq) {
+                                const uint32_t slot = bk * 4 + __ffs(eq) - 1;
+                                // t == s only when s lists itself (a data self-loop)
+                                if (!need_idx || HI[slot] != qoi[h]) {
+                                    ++cnt;
+                                    bs += HB[slot];
+                                }
+                                break;
+                            }
+                            if (kk.w == kFullMask) break;  // slots fill in order: an empty slot ends the chain
+                            bk = (bk + 1) & bmask;
+                        }
+                    }
+                    if (cnt) {
+                        hits += cnt;
+                        sum += (long long)cnt * ((long long)qa[h] - akc) + bs;
+                    }
+                }
+            }
+        }
+        local += (unsigned long long)sum;
+        local_c += hits;
+    };
+
     while (true) {
         uint32_t gi = 0;
         if (lane == 0) gi = past_deadline(rp, deadline) ? total : atomicAdd(cursor, 1u);
@@ -1065,8 +1319,16 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             for (uint32_t msk = sP.gt_mask; msk; msk &= msk - 1) lo = max(lo, my_m[__ffs(msk) - 1] + 1);
             for (uint32_t msk = sP.lt_mask; msk; msk &= msk - 1) hi = min(hi, my_m[__ffs(msk) - 1]);
             const uint32_t *mlist = g.adj + moff;
-            const uint32_t s0 = lo ? lbound(mlist, mdeg, lo) : 0;
-            const uint32_t e0 = hi != kFullMask ? lbound(mlist, mdeg, hi) : mdeg;
+            const uint32_t mu = njp ? my_m[sP.jpos[tmin]] : 0;  // the vertex whose list supplies S
+            const bool mdir = njp && sP.jdir[tmin];
+            const uint32_t s0 = lo ? lbound_own(g, mdir, mu, mlist, mdeg, lo, loops) : 0;
+            const uint32_t e0 = hi != kFullMask ? lbound_own(g, mdir, mu, mlist, mdeg, hi, loops) : mdeg;
+            // this lane's candidates rise, so its lower bounds in the first
+            // two other lists rise too: gallop from the last
+            uint32_t gp0 = 0, gp1 = 0;
+            // S goes to shared memory when the pair walk will read it (the
+            // other paths search S with global-memory loads)
+            uint32_t *const small = (MODE == kCountMode && walk_ok) ? tS[warp] : row;
             for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
                 const uint32_t x = x0 + lane;
                 bool ok = x < e0;
@@ -1078,13 +1340,29 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                     const uint2 o = g.out_info[v], i = g.in_info[v];
                     ok = i.y >= sP.qin && o.y >= sP.qout;
                 }
-                if (ok)
+                if (ok) {
+                    uint32_t r = 0;
                     for (uint32_t t = 0; t < njp; ++t) {
                         if (t == tmin) continue;
-                        if (!contains(g.adj + joff[warp][t], jdeg[warp][t], v)) { ok = false; break; }
+                        const uint32_t *lst = g.adj + joff[warp][t];
+                        const uint32_t len2 = jdeg[warp][t];
+                        if (r < 2) {
+                            const uint32_t pos = lbound_from(lst, len2, r == 0 ? gp0 : gp1, v);
+                            if (r == 0) gp0 = pos; else gp1 = pos;
+                            if (pos >= len2 || __ldg(lst + pos) != v) { ok = false; break; }
+                        } else if (!contains(lst, len2, v)) {
+                            ok = false;
+                            break;
+                        }
+                        ++r;
                     }
+                }
                 const unsigned m = __ballot_sync(kFullMask, ok);
-                if (ok) row[ns + __popc(m & lanemask_lt)] = v;
+                if (ok) {
+                    const uint32_t idx = ns + __popc(m & lanemask_lt);
+                    if (idx < kTS) small[idx] = v;
+                    else row[idx] = v;
+                }
                 ns += __popc(m);
                 if (MODE == kBytesMode && lane == 0) {
                     uint32_t per = 8;
@@ -1108,7 +1386,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 e = __shfl_sync(kFullMask, e, 0);
                 off = __shfl_sync(kFullMask, off, 0);
                 if (e != kFullMask) {
-                    for (uint32_t i = lane; i < ns; i += 32) big.pool[off + i] = row[i];
+                    for (uint32_t i = lane; i < ns; i += 32) big.pool[off + i] = i < kTS ? small[i] : row[i];
                     if (lane == 0) {
                         big.gi[e] = q0;
                         big.soff[e] = uint32_t(off);
@@ -1121,6 +1399,11 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             if (lane == 0) {
                 local_p += ns;
                 if (MODE == kBytesMode) local += 8ull * p + 8ull * njp + 4ull * ns;
+            }
+            if (MODE == kCountMode && walk_ok && ns > kTS) {
+                // the first kTS entries join the rest in the scratch row
+                for (uint32_t i = lane; i < kTS; i += 32) row[i] = small[i];
+                __syncwarp();
             }
         } else {
             S = big.pool + big.soff[b];
@@ -1140,7 +1423,11 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
         for (uint32_t msk = sC.gt_mask & below; msk; msk &= msk - 1) lo_c = max(lo_c, my_m[__ffs(msk) - 1] + 1);
         for (uint32_t msk = sC.lt_mask & below; msk; msk &= msk - 1) hi_c = min(hi_c, my_m[__ffs(msk) - 1]);
         if (!phase2) {
-            for (uint32_t i0 = 0; i0 < ns; i0 += 32) group(S, ns, i0, lo_c, hi_c);
+            if (MODE == kCountMode && walk_ok && ns <= kTS) {
+                pair_walk(ns, lo_c, hi_c);
+                __syncwarp();
+            } else
+                for (uint32_t i0 = 0; i0 < ns; i0 += 32) group(S, ns, i0, lo_c, hi_c);
         } else {
             group(S, ns, grp * 32, lo_c, hi_c);
         }
@@ -1403,6 +1690,7 @@ void device_graph_free(DeviceGraph *g) {
     if (g->in_info && g->in_info != g->out_info) cudaFree(g->in_info);
     cudaFree(g->out_info);
     cudaFree(g->adj);
+    cudaFree(g->bwd_out);
     cudaFree(g->d_u32);
     cudaFree(g->d_u64);
     cudaFree(g->d_plan);
@@ -1561,8 +1849,22 @@ struct Run {
         fb.pool_words = hp->fuse_pool_words;
         if (mode == kCountMode) CK(cudaMemsetAsync(fb.n, 0, 2 * sizeof(unsigned long long), g.stream));
         // CUTS_FUSE_SPLIT=<n> sets the deferral threshold (tests use small values)
-        uint32_t split = kBigS;
+        uint32_t split = g.fuse_split ? g.fuse_split : kBigS;
         if (const char *e = std::getenv("CUTS_FUSE_SPLIT")) split = uint32_t(std::strtoul(e, nullptr, 10));
+        // the phase-1 pair walk covers every fused plan except an extra list
+        // of c on p itself and a plain fold whose list or window moves with
+        // the vertex at p; CUTS_FUSE_WALK=0 turns it off (A/B comparisons)
+        uint32_t walk_ok = 1;
+        {
+            const LevelPlan &Lc = hp->plan.lv[p + 1];
+            const LevelPlan &Lf = hp->plan.lv[p + 2 < k ? p + 2 : p + 1];
+            for (uint32_t t = 0; t < Lc.nj; ++t)
+                if (((Lc.fuse_extra >> t) & 1u) && Lc.jpos[t] == p) walk_ok = 0;
+            if (Lc.fold && !Lf.ofold && (Lf.jpos[0] == p || (((Lf.gt_mask | Lf.lt_mask) >> p) & 1u))) walk_ok = 0;
+            if (g.max_deg >= (1u << 31)) walk_ok = 0;
+            const char *w = std::getenv("CUTS_FUSE_WALK");
+            if (w && w[0] == '0') walk_ok = 0;
+        }
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile) {
             CK(cudaEventCreate(&e0));
@@ -1571,19 +1873,19 @@ struct Run {
         }
         if (mode == kBytesMode) {
             k_fused<kBytesMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr);
+                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr, 0);
             CK(cudaGetLastError());
             res.launches++;
         } else {
             k_fused<kCountMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
+                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4, walk_ok);
             CK(cudaGetLastError());
             k_fused_scan<<<1, 1024, 0, g.stream>>>(fb);
             CK(cudaGetLastError());
             CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
             k_fused<kCountMode><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
                 view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64,
-                g.d_u64 + 3, g.d_u64 + 4);
+                g.d_u64 + 3, g.d_u64 + 4, 0);
             CK(cudaGetLastError());
             res.launches += 3;
         }
@@ -1863,7 +2165,7 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     uint64_t cap = 0;
     rc = prepare(g, q, opt.flags, k - 1, hp, dp, cap);
     if (rc) return rc;
-    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
+    Run run{g, graph_view(g), hp, dp, k, cap, 4, false, res};
     run.profile = opt.profile;
     run.budget_ms = opt.budget_ms;
     if (opt.budget_ms > 0) {  // the kernels' own deadline (device time from k_roots)
@@ -1936,7 +2238,7 @@ int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *line
     rc = prepare(g, q, CUTS_FLAG_NO_CLOSED_FORM, k, hp, dp, cap);
     if (rc) return rc;
     CountResult res;
-    Run run{g, DevView{g.out_info, g.in_info, g.adj, g.n}, hp, dp, k, cap, 4, false, res};
+    Run run{g, graph_view(g), hp, dp, k, cap, 4, false, res};
     run.dump = true;
     run.dump_file = f;
     run.query = &q;

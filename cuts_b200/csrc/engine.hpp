@@ -22,6 +22,10 @@ struct DeviceGraph {
     uint2 *in_info = nullptr;
     uint32_t *adj = nullptr;
     uint64_t adj_words = 0;
+    // per vertex: entries of its out- (in-) list below itself; bwd_in
+    // aliases bwd_out for a symmetric graph
+    uint32_t *bwd_out = nullptr;
+    uint32_t *bwd_in = nullptr;
     cudaStream_t stream = nullptr;
 
     // trie-level arena, carved per query
@@ -29,6 +33,7 @@ struct DeviceGraph {
     size_t arena_bytes = 0;
     size_t arena_default = 0;
     uint64_t level_cap_req = 0;   // 0 = automatic
+    uint32_t fuse_split = 0;      // fused count: |S| above which a parent is split (0 = default)
 
     // small device scratch and pinned host mirrors
     uint32_t *d_u32 = nullptr;             // counters / cursors / flags

@@ -160,6 +160,15 @@ __global__ void k_loops(uint32_t n, const uint2 *__restrict__ info, const uint32
     }
 }
 
+// bwd[d] = entries of d's list below d (a lower-bound search per vertex).
+__global__ void k_bwd(uint32_t n, const uint2 *__restrict__ info, const uint32_t *__restrict__ adj,
+                      uint32_t *__restrict__ bwd) {
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+        const uint2 inf = info[d];
+        bwd[d] = lbound(adj + inf.x, inf.y, d);
+    }
+}
+
 // Device buffers of one build, stream-ordered from the device's memory pool
 // (reused across builds instead of mapped and unmapped each time), released
 // on every exit.
@@ -345,6 +354,15 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     LCK(cudaGetLastError());
     if ((rc = read_flag())) return rc;
     g.loops = h_flag != 0;
+    // per-vertex counts of list entries below the vertex (windows that start
+    // or end at a list's own vertex need no search)
+    LCK(cudaMalloc(&g.bwd_out, sizeof(uint32_t) * std::max<uint32_t>(n, 1) * (symmetric ? 1 : 2)));
+    g.bwd_in = symmetric ? g.bwd_out : g.bwd_out + n;
+    if (n) {
+        k_bwd<<<grid, 256, 0, s>>>(n, g.out_info, g.adj, g.bwd_out);
+        if (!symmetric) k_bwd<<<grid, 256, 0, s>>>(n, g.in_info, g.adj, g.bwd_in);
+    }
+    LCK(cudaGetLastError());
     g.adj_words = total;
     g.symmetric = symmetric;
     g.n = n;

@@ -118,6 +118,13 @@ int cuts_graph_set_level_cap(cuts_graph g, uint64_t entries);
  * Frees the current arena; the next count allocates the new size. */
 int cuts_graph_set_arena_bytes(cuts_graph g, uint64_t bytes);
 
+/* Tile of the fused count of the last two levels: a parent whose candidate
+ * set S holds more than `split` vertices is split into groups of 32 handed
+ * to all warps (the hub split); 0 = the default (256, the size that fits
+ * one warp's shared-memory tile).  Replaces nothing in the reference, whose
+ * per-warp candidate tile is the fixed MAX_NE = 112 (common.h:31). */
+int cuts_graph_set_fuse_split(cuts_graph g, uint32_t split);
+
 void cuts_graph_free(cuts_graph g);
 
 /* ---- query graph -------------------------------------------------- */

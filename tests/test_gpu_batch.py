@@ -180,3 +180,22 @@ def test_batch_shards_partition_every_query():
         assert tot == full
     with pytest.raises(cb.CutsError):
         g.batch(qs).set_shard(3, 3)
+
+
+@pytest.mark.parametrize("name,flags", [("triangle", 0), ("4-clique+pendant", cb.FLAG_SYMMETRY_BREAK),
+                                        ("house", 0)])
+def test_count_autotuner(name, flags):
+    """The level engine's chunk / tile tuner: every configuration gives the
+    oracle's count, the best one is kept on the graph and reproduces it."""
+    from cuts_b200 import autotune
+    from oracle import oracle as O
+    from tests.helpers import oracle_graph_from_host
+    h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
+    g = h.upload(0)
+    k, arcs = cb.named_query_arcs(name)
+    q = cb.Query.from_arcs(k, arcs)
+    best, times = autotune.tune_count(g, q, flags=flags, chunks=(1, 3), splits=(8, 64, 256),
+                                      level_caps=(0, 4096), reps=2)
+    assert len(times) == 2 * 3 * 2 and best in times and times[best] == min(times.values())
+    want = O.count(oracle_graph_from_host(h), O.Graph.from_arcs(k, arcs), q.order)[0]
+    assert g.count(q, chunks=best[0], flags=flags).count == want
