@@ -778,7 +778,8 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
             return set_error(CUTS_ERR_CUDA, "cuts_count_noalloc: plan upload failed");
     }
     const DevView view{reinterpret_cast<const uint2 *>(info_out),
-                       reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n, nullptr, nullptr};
+                       reinterpret_cast<const uint2 *>(sym ? info_out : info_in), adj, n, nullptr, nullptr,
+                       nullptr, 0};
     const unsigned long long total = (unsigned long long)nq * n;
     const uint32_t grid = uint32_t(std::min<unsigned long long>(blocks, (total + kBW - 1) / kBW));
     k_batch_noalloc<<<std::max<uint32_t>(grid, 1), kBW * 32, 0, stream>>>(view, sc, nq, counts);

@@ -18,12 +18,20 @@ struct DevView {
     // (may be null: the lists are searched instead)
     const uint32_t *bwd_out;
     const uint32_t *bwd_in;
+    // dense core of a symmetric graph: the kCore vertices of highest id
+    // (the hubs, ids being degree ranks), from core0 up; row d - core0 of
+    // core_bits (kCore / 32 words) has bit u - core0 set when d lists u.
+    // Null when absent.
+    const uint32_t *core_bits;
+    uint32_t core0;
 };
+
+constexpr uint32_t kCore = 1024;  // vertices in the dense core
 
 // The kernels' view of a resident graph (a DeviceGraph).
 template <class G>
 inline DevView graph_view(const G &g) {
-    return DevView{g.out_info, g.in_info, g.adj, g.n, g.bwd_out, g.bwd_in};
+    return DevView{g.out_info, g.in_info, g.adj, g.n, g.bwd_out, g.bwd_in, g.core_bits, g.core0};
 }
 
 __device__ __forceinline__ uint32_t lbound(const uint32_t *__restrict__ a, uint32_t len,

@@ -710,14 +710,18 @@ struct FusedBig {
 constexpr uint32_t kTS = 256;
 constexpr uint32_t kHS = 512;  // hash slots of the admissible t, buckets of 4 (load at most 1/2)
 
-// 8 resident blocks (32 warps) per SM at up to 64 registers: the pair walk
-// keeps its row state in registers
-template <int MODE>
-__global__ void __launch_bounds__(kZW * 32, 8)
+// WALK instances (phase 1 of plans the pair walk covers): 8 resident blocks
+// (32 warps) per SM at up to 64 registers -- the walk keeps its row state
+// in registers and ~25 KB of tables in shared memory.  The others: 12
+// resident blocks (48 warps) at 40 registers -- they wait on dependent L2
+// loads, and the extra warps outweigh the spills that cap costs.
+template <int MODE, bool WALK>
+__global__ void __launch_bounds__(kZW * 32, WALK ? 8 : 12)
 k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb, uint32_t phase,
         uint32_t split, uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride, FusedBig big,
         unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,
-        unsigned long long *__restrict__ acc_p, uint32_t walk_ok) {
+        unsigned long long *__restrict__ acc_p) {
+    constexpr bool walk_ok = WALK && MODE == kCountMode;
     __shared__ LevelPlan sP, sC, sF;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
@@ -726,10 +730,12 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
     __shared__ uint32_t xoff[kZW][kMaxJ], xdeg[kZW][kMaxJ];
     // the pair walk's per-parent tables: S, and a hash table of the vertices
     // admissible as t (keys in buckets of 4, their index in S and term B)
-    __shared__ uint32_t tS[MODE == kCountMode ? kZW : 1][kTS];
-    __shared__ uint4 tHK[MODE == kCountMode ? kZW : 1][kHS / 4];
-    __shared__ uint8_t tHI[MODE == kCountMode ? kZW : 1][kHS];
-    __shared__ int32_t tHB[MODE == kCountMode ? kZW : 1][kHS];
+    __shared__ uint32_t tS[walk_ok ? kZW : 1][kTS];
+    __shared__ uint4 tHK[walk_ok ? kZW : 1][kHS / 4];
+    // dense core: the admissible t of S as bits of the core (per warp)
+    __shared__ uint32_t tSV[walk_ok ? kZW : 1][kCore / 32];
+    __shared__ uint8_t tHI[walk_ok ? kZW : 1][kHS];
+    __shared__ int32_t tHB[walk_ok ? kZW : 1][kHS];
     {
         const uint32_t words = sizeof(LevelPlan) / 4;
         const uint32_t c = p + 1;
@@ -752,6 +758,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
     const uint32_t lanemask_lt = (1u << lane) - 1;
     uint32_t *my_m = wm[warp];
     uint32_t *const row = scratch + size_t(blockIdx.x * kZW + warp) * stride;
+
     const uint32_t c = p + 1;
     // the counted level c is folded when level c carries the fold flag
     const bool cfold = sC.fold != 0;
@@ -1089,7 +1096,17 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
         uint8_t *const HI = tHI[warp];
         int32_t *const HB = tHB[warp];
         const bool need_idx = !c_gt_s && !c_lt_s && loops;
-        for (uint32_t x = lane; x <= bmask; x += 32) HK4[x] = make_uint4(kFullMask, kFullMask, kFullMask, kFullMask);
+        // dense core path for rows s in the core: every t > s is then in the
+        // core too, and s's pairs are popcounts of its bitmap row against
+        // the admissible t (needs t > s, no extra lists, and B(t) from t's
+        // degree alone)
+        const bool core_rows = g.core_bits && c_gt_s && !extra && (!cfold || (sF.ofold && !loops));
+        // the table serves rows below the core only
+        const bool table = !core_rows || S[0] < g.core0;
+        uint32_t *const SV = tSV[warp];
+        if (core_rows) SV[lane] = 0;
+        if (table)
+            for (uint32_t x = lane; x <= bmask; x += 32) HK4[x] = make_uint4(kFullMask, kFullMask, kFullMask, kFullMask);
         __syncwarp();
         // the admissible t, with B(t), into the table
         uint32_t nv = 0;
@@ -1108,7 +1125,11 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                     ok = i2.y >= sC.qin && o.y >= sC.qout;
                 }
             }
-            if (ok) {
+            if (ok && core_rows && v >= g.core0) {
+                const uint32_t u = v - g.core0;
+                atomicOr(&SV[u >> 5], 1u << (u & 31));
+            }
+            if (ok && table) {
                 int32_t b = 0;
                 if (c_in_orbit) {
                     const uint2 vi = sF.jdir[0] ? g.in_info[v] : g.out_info[v];
@@ -1145,18 +1166,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             uint32_t ea = 0, eb = 0, nq = 0, arow = 1;
             if (i < ns) {
                 const uint32_t sv = S[i];
-                const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
-                const uint32_t *Ls = g.adj + is.x;
-                uint32_t lo_v = lo_c, hi_v = hi_c;
-                if (c_gt_s) lo_v = max(lo_v, sv + 1);
-                if (c_lt_s) hi_v = min(hi_v, sv);
-                const bool sdir = sC.jdir[tp] != 0;
-                const uint32_t p0 = lo_v ? lbound_own(g, sdir, sv, Ls, is.y, lo_v, loops) : 0;
-                const uint32_t p1 = hi_v != kFullMask ? lbound_own(g, sdir, sv, Ls, is.y, hi_v, loops) : is.y;
-                if (p1 > p0) {
-                    ea = is.x + p0;
-                    eb = is.x + p1;
-                    nq = ((eb + 3) >> 2) - (ea >> 2);
+                {
                     // A(s): the orbit base with s at p (orbit_base's sum, the
                     // parent's part computed once), or the plain fold's base
                     if (cfold && sF.ofold) {
@@ -1182,6 +1192,48 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                         const bool in = sv >= f_lo && sv < f_hi &&
                                         (((sF.guar_mask >> p) & 1u) || contains(g.adj + f_off, f_deg, sv));
                         arow = (f_we > f_ws ? f_we - f_ws : 0) - f_sub - (in ? 1u : 0u);
+                    }
+                }
+                if (core_rows && sv >= g.core0) {
+                    // a core row: t ranges over the admissible core bits
+                    // above s in s's bitmap row
+                    const uint32_t si = sv - g.core0;
+                    const uint4 *rowp = reinterpret_cast<const uint4 *>(g.core_bits + size_t(si) * (kCore / 32));
+                    const uint32_t w0 = si >> 5;
+                    uint32_t cnt = 0;
+                    long long dsum = 0;
+                    for (uint32_t q = w0 >> 2; q < kCore / 128; ++q) {
+                        const uint4 r4 = __ldg(rowp + q);
+                        const uint32_t rw[4] = {r4.x, r4.y, r4.z, r4.w};
+                        #pragma unroll
+                        for (uint32_t k = 0; k < 4; ++k) {
+                            const uint32_t j = 4 * q + k;
+                            if (j < w0) continue;
+                            uint32_t w = rw[k] & SV[j];
+                            if (j == w0) w &= ~((2u << (si & 31)) - 1u);
+                            cnt += __popc(w);
+                            if (c_in_orbit)
+                                for (; w; w &= w - 1) dsum += g.out_info[g.core0 + 32 * j + __ffs(w) - 1].y;
+                        }
+                    }
+                    if (cnt) {
+                        hits += cnt;
+                        // B(t) = |L(t)| - c for the orbit fold's pendant (no self-loops here)
+                        sum += (long long)cnt * ((long long)arow - akc) + (c_in_orbit ? dsum - (long long)cnt * c : 0);
+                    }
+                } else {
+                    const uint2 is = sC.jdir[tp] ? g.in_info[sv] : g.out_info[sv];
+                    const uint32_t *Ls = g.adj + is.x;
+                    uint32_t lo_v = lo_c, hi_v = hi_c;
+                    if (c_gt_s) lo_v = max(lo_v, sv + 1);
+                    if (c_lt_s) hi_v = min(hi_v, sv);
+                    const bool sdir = sC.jdir[tp] != 0;
+                    const uint32_t p0 = lo_v ? lbound_own(g, sdir, sv, Ls, is.y, lo_v, loops) : 0;
+                    const uint32_t p1 = hi_v != kFullMask ? lbound_own(g, sdir, sv, Ls, is.y, hi_v, loops) : is.y;
+                    if (p1 > p0) {
+                        ea = is.x + p0;
+                        eb = is.x + p1;
+                        nq = ((eb + 3) >> 2) - (ea >> 2);
                     }
                 }
             }
@@ -1328,7 +1380,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             uint32_t gp0 = 0, gp1 = 0;
             // S goes to shared memory when the pair walk will read it (the
             // other paths search S with global-memory loads)
-            uint32_t *const small = (MODE == kCountMode && walk_ok) ? tS[warp] : row;
+            uint32_t *const small = walk_ok ? tS[warp] : row;
             for (uint32_t x0 = s0; x0 < e0; x0 += 32) {
                 const uint32_t x = x0 + lane;
                 bool ok = x < e0;
@@ -1400,7 +1452,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 local_p += ns;
                 if (MODE == kBytesMode) local += 8ull * p + 8ull * njp + 4ull * ns;
             }
-            if (MODE == kCountMode && walk_ok && ns > kTS) {
+            if (walk_ok && ns > kTS) {
                 // the first kTS entries join the rest in the scratch row
                 for (uint32_t i = lane; i < kTS; i += 32) row[i] = small[i];
                 __syncwarp();
@@ -1423,8 +1475,8 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
         for (uint32_t msk = sC.gt_mask & below; msk; msk &= msk - 1) lo_c = max(lo_c, my_m[__ffs(msk) - 1] + 1);
         for (uint32_t msk = sC.lt_mask & below; msk; msk &= msk - 1) hi_c = min(hi_c, my_m[__ffs(msk) - 1]);
         if (!phase2) {
-            if (MODE == kCountMode && walk_ok && ns <= kTS) {
-                pair_walk(ns, lo_c, hi_c);
+            if (walk_ok && ns <= kTS) {
+                if constexpr (walk_ok) pair_walk(ns, lo_c, hi_c);
                 __syncwarp();
             } else
                 for (uint32_t i0 = 0; i0 < ns; i0 += 32) group(S, ns, i0, lo_c, hi_c);
@@ -1581,6 +1633,7 @@ int g_num_sms = 0;
 int g_level_blocks[3] = {0, 0, 0};
 int g_flat_blocks[3] = {0, 0, 0};
 int g_fused_blocks[3] = {0, 0, 0};
+int g_fused_walk_blocks = 0;
 // CUTS_LEVEL_KERNEL=warp selects the warp-per-parent form (A/B comparisons)
 bool g_use_flat = true;
 
@@ -1602,10 +1655,12 @@ int launch_geometry() {
     g_flat_blocks[kCountMode] = std::max(1, b) * g_num_sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_level_flat<kBytesMode>, kFW * 32, 0));
     g_flat_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kCountMode>, kZW * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kCountMode, false>, kZW * 32, 0));
     g_fused_blocks[kCountMode] = std::max(1, b) * g_num_sms;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kBytesMode>, kZW * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kBytesMode, false>, kZW * 32, 0));
     g_fused_blocks[kBytesMode] = std::max(1, b) * g_num_sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused<kCountMode, true>, kZW * 32, 0));
+    g_fused_walk_blocks = std::max(1, b) * g_num_sms;
     const char *kv = std::getenv("CUTS_LEVEL_KERNEL");
     g_use_flat = !(kv && std::strcmp(kv, "warp") == 0);
     return CUTS_OK;
@@ -1691,6 +1746,7 @@ void device_graph_free(DeviceGraph *g) {
     cudaFree(g->out_info);
     cudaFree(g->adj);
     cudaFree(g->bwd_out);
+    cudaFree(g->core_bits);
     cudaFree(g->d_u32);
     cudaFree(g->d_u64);
     cudaFree(g->d_plan);
@@ -1836,8 +1892,8 @@ struct Run {
     // deferred and phase 2 over their groups.
     int launch_fused(int mode, uint32_t p, uint32_t pa, uint32_t pb) {
         CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
-        const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_blocks[mode]),
-                                                                         (pb - pa + kZW - 1) / kZW));
+        uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_blocks[mode]),
+                                                                   (pb - pa + kZW - 1) / kZW));
         FusedBig fb;
         fb.n = reinterpret_cast<unsigned long long *>(hp->fuse_big);
         fb.cap = hp->fuse_big_cap;
@@ -1851,13 +1907,19 @@ struct Run {
         // CUTS_FUSE_SPLIT=<n> sets the deferral threshold (tests use small values)
         uint32_t split = g.fuse_split ? g.fuse_split : kBigS;
         if (const char *e = std::getenv("CUTS_FUSE_SPLIT")) split = uint32_t(std::strtoul(e, nullptr, 10));
-        // the phase-1 pair walk covers every fused plan except an extra list
-        // of c on p itself and a plain fold whose list or window moves with
-        // the vertex at p; CUTS_FUSE_WALK=0 turns it off (A/B comparisons)
+        // the phase-1 pair walk covers the fused plans that order the
+        // vertices at p and c (symmetry breaking: each pair of S once, and a
+        // row's list window starts or ends at s), except an extra list of c
+        // on p itself and a plain fold whose list or window moves with the
+        // vertex at p; a plan without that order (every ordered pair, so a
+        // row's window is s's whole list) keeps the per-pair intersection,
+        // which iterates the shorter side.  CUTS_FUSE_WALK=0 turns the walk
+        // off (A/B comparisons)
         uint32_t walk_ok = 1;
         {
             const LevelPlan &Lc = hp->plan.lv[p + 1];
             const LevelPlan &Lf = hp->plan.lv[p + 2 < k ? p + 2 : p + 1];
+            if (!(((Lc.gt_mask | Lc.lt_mask) >> p) & 1u)) walk_ok = 0;
             for (uint32_t t = 0; t < Lc.nj; ++t)
                 if (((Lc.fuse_extra >> t) & 1u) && Lc.jpos[t] == p) walk_ok = 0;
             if (Lc.fold && !Lf.ofold && (Lf.jpos[0] == p || (((Lf.gt_mask | Lf.lt_mask) >> p) & 1u))) walk_ok = 0;
@@ -1872,20 +1934,26 @@ struct Run {
             CK(cudaEventRecord(e0, g.stream));
         }
         if (mode == kBytesMode) {
-            k_fused<kBytesMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr, 0);
+            k_fused<kBytesMode, false><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
+                g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr);
             CK(cudaGetLastError());
             res.launches++;
         } else {
-            k_fused<kCountMode><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split, g.d_u32 + kSlotCursor,
-                hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4, walk_ok);
+            if (walk_ok) {
+                blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_walk_blocks), (pb - pa + kZW - 1) / kZW));
+                k_fused<kCountMode, true><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
+                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
+            } else {
+                k_fused<kCountMode, false><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
+                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
+            }
             CK(cudaGetLastError());
             k_fused_scan<<<1, 1024, 0, g.stream>>>(fb);
             CK(cudaGetLastError());
             CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
-            k_fused<kCountMode><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
+            k_fused<kCountMode, false><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
                 view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64,
-                g.d_u64 + 3, g.d_u64 + 4, 0);
+                g.d_u64 + 3, g.d_u64 + 4);
             CK(cudaGetLastError());
             res.launches += 3;
         }

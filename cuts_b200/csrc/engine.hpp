@@ -26,6 +26,10 @@ struct DeviceGraph {
     // aliases bwd_out for a symmetric graph
     uint32_t *bwd_out = nullptr;
     uint32_t *bwd_in = nullptr;
+    // adjacency bitmap of the highest-id vertices (symmetric graphs): row
+    // d - core0, bit u - core0 (kCore x kCore bits)
+    uint32_t *core_bits = nullptr;
+    uint32_t core0 = 0;
     cudaStream_t stream = nullptr;
 
     // trie-level arena, carved per query

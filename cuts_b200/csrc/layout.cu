@@ -169,6 +169,23 @@ __global__ void k_bwd(uint32_t n, const uint2 *__restrict__ info, const uint32_t
     }
 }
 
+// Dense core rows: one warp per core vertex d, its list entries u >= core0
+// set bit u - core0 of row d - core0 (rows are zeroed before).
+__global__ void k_core_bits(uint32_t n, uint32_t core0, const uint2 *__restrict__ info,
+                            const uint32_t *__restrict__ adj, uint32_t *__restrict__ bits) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t words = kCore / 32;
+    for (uint32_t d = core0 + (blockIdx.x * blockDim.x + threadIdx.x) / 32; d < n;
+         d += (gridDim.x * blockDim.x) / 32) {
+        const uint2 inf = info[d];
+        const uint32_t *l = adj + inf.x;
+        for (uint32_t i = lbound(l, inf.y, core0) + lane; i < inf.y; i += 32) {
+            const uint32_t u = l[i] - core0;
+            atomicOr(bits + size_t(d - core0) * words + (u >> 5), 1u << (u & 31));
+        }
+    }
+}
+
 // Device buffers of one build, stream-ordered from the device's memory pool
 // (reused across builds instead of mapped and unmapped each time), released
 // on every exit.
@@ -363,6 +380,16 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
         if (!symmetric) k_bwd<<<grid, 256, 0, s>>>(n, g.in_info, g.adj, g.bwd_in);
     }
     LCK(cudaGetLastError());
+    if (symmetric && n) {
+        // the dense core: the kCore highest ids (the hubs under the degree
+        // ranking), as an adjacency bitmap
+        g.core0 = n > kCore ? n - kCore : 0;
+        const size_t words = size_t(kCore) * (kCore / 32);
+        LCK(cudaMalloc(&g.core_bits, words * sizeof(uint32_t)));
+        LCK(cudaMemsetAsync(g.core_bits, 0, words * sizeof(uint32_t), s));
+        k_core_bits<<<(kCore * 32 + 255) / 256, 256, 0, s>>>(n, g.core0, g.out_info, g.adj, g.core_bits);
+        LCK(cudaGetLastError());
+    }
     g.adj_words = total;
     g.symmetric = symmetric;
     g.n = n;

@@ -33,10 +33,11 @@ _ORACLE = {}
 
 
 def oracle_count(od, k, arcs, order):
+    # the entry keeps its graph alive, so an id is never reused for another graph
     key = (id(od), k, tuple(arcs), tuple(order))
-    if key not in _ORACLE:
-        _ORACLE[key] = O.count(od, O.Graph.from_arcs(k, arcs), order)
-    return _ORACLE[key]
+    if key not in _ORACLE or _ORACLE[key][0] is not od:
+        _ORACLE[key] = (od, O.count(od, O.Graph.from_arcs(k, arcs), order))
+    return _ORACLE[key][1]
 
 
 def _check(g, od, k, arcs, flags=0, chunks=1, levels=True):
