@@ -90,6 +90,7 @@ _SIGS = {
                                      _u64p, C.POINTER(C.c_float), _u64p]),
     "cuts_count_sharded_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                         _u64p, _fp, _u64p, _u64p]),
+    "cuts_dump_sharded": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_char_p, _u64p]),
     "cuts_dump": (C.c_int, [_vp, _vp, C.c_char_p, _u64p]),
     "cuts_search": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, _u64p,
                               C.POINTER(C.c_float)]),
@@ -468,9 +469,14 @@ class Graph:
         _check(rc)
         return CountResult(cnt.value, ms.value, [int(x) for x in lv]), True
 
-    def dump(self, q: Query, path: str) -> int:
+    def dump(self, q: Query, path: str, shard: int = 0, nshards: int = 1) -> int:
+        """Write ans.txt lines (the matches whose root is in the stripe
+        u % nshards == shard); returns the number of lines."""
         n = C.c_uint64()
-        _check(lib().cuts_dump(self._h, q._h, path.encode(), C.byref(n)))
+        if nshards == 1:
+            _check(lib().cuts_dump(self._h, q._h, path.encode(), C.byref(n)))
+        else:
+            _check(lib().cuts_dump_sharded(self._h, q._h, shard, nshards, path.encode(), C.byref(n)))
         return n.value
 
     def count_batch(self, queries: Sequence[Query], flags: int = 0):

@@ -416,6 +416,12 @@ int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count) {
     GUARD(device_dump(*g->dev, q->q, path, count));
 }
 
+int cuts_dump_sharded(cuts_graph g, cuts_query q, uint32_t shard, uint32_t nshards, const char *path,
+                      uint64_t *count) {
+    if (!g || !g->dev || !q || !path) return set_error(CUTS_ERR_ARG, "null argument");
+    GUARD(device_dump(*g->dev, q->q, path, count, shard, nshards));
+}
+
 static std::string base_name(const std::string &s) {
     // common.cpp:19-26: the part after the last '/', or "" without one
     size_t i = s.rfind('/');

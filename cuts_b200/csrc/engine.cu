@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <charconv>
 #include <chrono>
 #include <climits>
@@ -32,6 +33,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
+#include <omp.h>
 
 #include "device_util.cuh"
 #include "engine.hpp"
@@ -56,6 +59,10 @@ constexpr uint32_t kTile = 256; // planner tile (parents)
 struct RunParams {
     Plan plan;
     uint32_t stored;   // levels kept in HBM: k-1 when counting, k when dumping
+    // level whose entries keep, in their ub slot, the adj offset their vertex
+    // was drawn from (the last stored level before a fused count: its child
+    // bound is never read); kFull = none
+    uint32_t pos_lvl;
     uint32_t fuse_stride;  // words per warp row of the fused kernel's scratch
     uint32_t *fuse_scratch;
     uint32_t *fuse_big;    // the fused kernel's deferred parents (counters, arrays, pool)
@@ -197,14 +204,16 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
     uint32_t *my_m = wm[warp];
     const uint32_t k = s_k;
     const bool sym = s_sym != 0;
-    // entries of L_lvl need a child bound when level lvl+1 is stored too
-    const bool need_ub = MODE == kExpand && lvl + 1 < s_stored;
+    // entries of L_lvl need a child bound when level lvl+1 is stored too; at
+    // the position level the slot keeps where the vertex sits in its list
+    const bool store_pos = MODE == kExpand && lvl == rp->pos_lvl;
+    const bool need_ub = (MODE == kExpand && lvl + 1 < s_stored) || store_pos;
     uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
     uint32_t *out_p = MODE == kExpand ? rp->par[lvl] : nullptr;
     uint32_t *out_u = MODE == kExpand ? rp->ub[lvl] : nullptr;
     // next-level joins on the child itself (position lvl) bound its children
     bool ub_out = false, ub_in = false;
-    if (need_ub)
+    if (need_ub && !store_pos)
         for (uint32_t t = 0; t < sN.nj; ++t)
             if (sN.jpos[t] == lvl) (sN.jdir[t] ? ub_in : ub_out) = true;
     const uint32_t nj = sL.nj;
@@ -350,6 +359,7 @@ k_level(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, 
                     uint32_t ub = ubp;
                     if (ub_out) ub = min(ub, co.y);
                     if (ub_in) ub = min(ub, ci.y);
+                    if (store_pos) ub = moff + x;
                     const unsigned m = __ballot_sync(kFull, ok);
                     const uint32_t nn = __popc(m);
                     if (obn + nn > uint32_t(kOutBuf)) flush();
@@ -424,12 +434,13 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lanemask_lt = (1u << lane) - 1;
     const bool sym = s_sym != 0;
-    const bool need_ub = MODE == kExpand && lvl + 1 < s_stored;
+    const bool store_pos = MODE == kExpand && lvl == rp->pos_lvl;
+    const bool need_ub = (MODE == kExpand && lvl + 1 < s_stored) || store_pos;
     uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
     uint32_t *out_p = MODE == kExpand ? rp->par[lvl] : nullptr;
     uint32_t *out_u = MODE == kExpand ? rp->ub[lvl] : nullptr;
     bool ub_out = false, ub_in = false;
-    if (need_ub)
+    if (need_ub && !store_pos)
         for (uint32_t t = 0; t < sN.nj; ++t)
             if (sN.jpos[t] == lvl) (sN.jdir[t] ? ub_in : ub_out) = true;
     const uint32_t nj = sL.nj;
@@ -647,6 +658,7 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                 uint32_t ub = o_ubp;
                 if (ub_out) ub = min(ub, co.y);
                 if (ub_in) ub = min(ub, ci.y);
+                if (store_pos) ub = o_moff + idx;  // where c sits in the list it came from
                 const unsigned m = __ballot_sync(kFullMask, ok);
                 const uint32_t nn = __popc(m);
                 if (obn + nn > uint32_t(kOutBuf)) flush();
@@ -715,13 +727,17 @@ constexpr uint32_t kHS = 512;  // hash slots of the admissible t, buckets of 4 (
 // in registers and ~25 KB of tables in shared memory.  The others: 12
 // resident blocks (48 warps) at 40 registers -- they wait on dependent L2
 // loads, and the extra warps outweigh the spills that cap costs.
-template <int MODE, bool WALK>
+template <int MODE, bool WALK, bool TALLY = false>
 __global__ void __launch_bounds__(kZW * 32, WALK ? 8 : 12)
 k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, uint32_t pb, uint32_t phase,
         uint32_t split, uint32_t *__restrict__ cursor, uint32_t *__restrict__ scratch, uint32_t stride, FusedBig big,
         unsigned long long *__restrict__ acc, unsigned long long *__restrict__ acc_c,
-        unsigned long long *__restrict__ acc_p) {
+        unsigned long long *__restrict__ acc_p, unsigned long long *__restrict__ acc_bytes) {
     constexpr bool walk_ok = WALK && MODE == kCountMode;
+    // TALLY: also add the bytes this count reads from global memory to
+    // *acc_bytes (the last level's algorithmic traffic; counts go to scratch)
+    constexpr bool tally = TALLY && MODE == kCountMode;
+    unsigned long long tb = 0;
     __shared__ LevelPlan sP, sC, sF;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
@@ -843,9 +859,13 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                     }
                     fbase = (we > ws ? we - ws : 0) - sub;
                 }
-                if (MODE == kBytesMode)
-                    local += 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iters ? ds : nS) +
-                             (sig_c ? 8ull * nit : 0) + (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
+                if (MODE == kBytesMode || tally) {
+                    const unsigned long long by = 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iters ? ds : nS) +
+                                                  (sig_c ? 8ull * nit : 0) +
+                                                  (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
+                    if (MODE == kBytesMode) local += by;
+                    else tb += by;
+                }
             }
             if (MODE == kBytesMode) return;
             uint32_t incl = nit;
@@ -979,11 +999,14 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             const uint32_t nS = te - ts, nL = ls1 > ls0 ? ls1 - ls0 : 0;
             const bool iterS = nS <= nL;
             const uint32_t nit = iterS ? nS : nL;
-            if (MODE == kBytesMode) {
-                if (lane == 0)
-                    local += 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iterS ? ds : nS) +
-                             (sig_c ? 8ull * nit : 0) + (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
-                continue;
+            if (MODE == kBytesMode || tally) {
+                const unsigned long long by = 12 + 4ull * nit + uint64_t(nit) * 4 * probes(iterS ? ds : nS) +
+                                              (sig_c ? 8ull * nit : 0) + (cfold ? 8 + 4ull * (p + 1) * probes(fdeg) : 0);
+                if (lane == 0) {
+                    if (MODE == kBytesMode) local += by;
+                    else tb += by;
+                }
+                if (MODE == kBytesMode) continue;
             }
             uint32_t gal = iterS ? ls0 : ts;
             for (uint32_t y0 = 0; y0 < nit; y0 += 32) {
@@ -1132,6 +1155,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             if (ok && table) {
                 int32_t b = 0;
                 if (c_in_orbit) {
+                    if (tally) tb += 8;
                     const uint2 vi = sF.jdir[0] ? g.in_info[v] : g.out_info[v];
                     b = int32_t(vi.y) - int32_t(c) - ((loops && contains(g.adj + vi.x, vi.y, v)) ? 1 : 0);
                 } else if (cfold && !sF.ofold) {
@@ -1216,6 +1240,9 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                                 for (; w; w &= w - 1) dsum += g.out_info[g.core0 + 32 * j + __ffs(w) - 1].y;
                         }
                     }
+                    // the row's bitmap words from s's own word on, and t's
+                    // degree per hit (orbit fold)
+                    if (tally) tb += 8 + 16ull * (kCore / 128 - (w0 >> 2)) + (c_in_orbit ? 8ull * cnt : 0);
                     if (cnt) {
                         hits += cnt;
                         // B(t) = |L(t)| - c for the orbit fold's pendant (no self-loops here)
@@ -1235,6 +1262,8 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                         eb = is.x + p1;
                         nq = ((eb + 3) >> 2) - (ea >> 2);
                     }
+                    // s's info, its window bound, the window's quads
+                    if (tally) tb += 12 + 16ull * nq;
                 }
             }
             uint32_t incl = nq;
@@ -1373,7 +1402,14 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             const uint32_t *mlist = g.adj + moff;
             const uint32_t mu = njp ? my_m[sP.jpos[tmin]] : 0;  // the vertex whose list supplies S
             const bool mdir = njp && sP.jdir[tmin];
-            const uint32_t s0 = lo ? lbound_own(g, mdir, mu, mlist, mdeg, lo, loops) : 0;
+            uint32_t s0 = kFullMask;
+            if (lo && p >= 2 && rp->pos_lvl == p - 1 && lo == my_m[p - 1] + 1) {
+                // the window starts right after the parent's own vertex: when
+                // that vertex was drawn from this very list, its offset is known
+                const uint32_t apos = rp->ub[p - 1][q0];
+                if (apos >= moff && apos - moff < mdeg) s0 = apos - moff + 1;
+            }
+            if (s0 == kFullMask) s0 = lo ? lbound_own(g, mdir, mu, mlist, mdeg, lo, loops) : 0;
             const uint32_t e0 = hi != kFullMask ? lbound_own(g, mdir, mu, mlist, mdeg, hi, loops) : mdeg;
             // this lane's candidates rise, so its lower bounds in the first
             // two other lists rise too: gallop from the last
@@ -1416,14 +1452,17 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                     else row[idx] = v;
                 }
                 ns += __popc(m);
-                if (MODE == kBytesMode && lane == 0) {
+                if ((MODE == kBytesMode || tally) && lane == 0) {
                     uint32_t per = 8;
                     for (uint32_t t = 0; t < njp; ++t)
                         if (t != tmin) per += 4 * probes(jdeg[warp][t]);
-                    local += 4ull * min(32u, e0 - x0) + uint64_t(min(32u, e0 - x0)) * per;
+                    const unsigned long long by = 4ull * min(32u, e0 - x0) + uint64_t(min(32u, e0 - x0)) * per;
+                    if (MODE == kBytesMode) local += by;
+                    else tb += by;
                 }
             }
             __syncwarp();
+            if (tally && lane == 0) tb += 8ull * p + 8ull * njp + 4ull * ns;
             if (MODE == kCountMode && ns > split) {
                 // defer: save S in the pool for phase 2 (or keep it here when full)
                 unsigned long long off = 0;
@@ -1495,6 +1534,11 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
             if (local_c) atomicAdd(acc_c, local_c);
             if (local_p) atomicAdd(acc_p, local_p);
         }
+    }
+    if (tally) {
+        #pragma unroll
+        for (int o = 16; o; o >>= 1) tb += __shfl_xor_sync(kFullMask, tb, o);
+        if (lane == 0 && tb) atomicAdd(acc_bytes, tb);
     }
 }
 
@@ -1669,6 +1713,8 @@ int launch_geometry() {
 // u32 scratch slots
 enum : int { kSlotN0 = 0, kSlotErr = 1, kSlotNb = 2, kSlotOver = 3, kSlotOut = 8, kSlotCursor = 32, kSlots = 64 };
 constexpr int kU64Stamp = 5;  // d_u64 slot: device clock at the start of a budgeted run
+constexpr int kU64Scratch = 8;  // d_u64 slots 8..10: counts of the bytes pass (discarded)
+constexpr int kU64Slots = 16;
 
 }  // namespace
 
@@ -1705,10 +1751,10 @@ static int device_graph_build(uint32_t n, const uint64_t *out_off, const uint32_
         return rc;
     }
     if ((e = cudaMalloc(&g->d_u32, sizeof(uint32_t) * kSlots))) return fail(e, "scratch");
-    if ((e = cudaMalloc(&g->d_u64, sizeof(unsigned long long) * 8))) return fail(e, "scratch");
+    if ((e = cudaMalloc(&g->d_u64, sizeof(unsigned long long) * kU64Slots))) return fail(e, "scratch");
     if ((e = cudaMalloc(&g->d_plan, sizeof(RunParams)))) return fail(e, "scratch");
     if ((e = cudaMallocHost(&g->h_u32, sizeof(uint32_t) * kSlots))) return fail(e, "pinned");
-    if ((e = cudaMallocHost(&g->h_u64, sizeof(unsigned long long) * 8))) return fail(e, "pinned");
+    if ((e = cudaMallocHost(&g->h_u64, sizeof(unsigned long long) * kU64Slots))) return fail(e, "pinned");
     if ((e = cudaMallocHost(&g->h_plan, sizeof(RunParams)))) return fail(e, "pinned");
     if ((e = cudaEventCreate(&g->ev0)) || (e = cudaEventCreate(&g->ev1))) return fail(e, "event");
     if ((e = cudaStreamSynchronize(g->stream))) return fail(e, "upload sync");
@@ -1933,27 +1979,44 @@ struct Run {
             CK(cudaEventCreate(&e1));
             CK(cudaEventRecord(e0, g.stream));
         }
-        if (mode == kBytesMode) {
+        if (mode == kBytesMode && !walk_ok) {
             k_fused<kBytesMode, false><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
-                g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr);
+                g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64 + 2, nullptr, nullptr,
+                nullptr);
             CK(cudaGetLastError());
             res.launches++;
         } else {
-            if (walk_ok) {
-                blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_walk_blocks), (pb - pa + kZW - 1) / kZW));
-                k_fused<kCountMode, true><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
-                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
-            } else {
+            // counting; the bytes pass of a walk plan runs the same launches
+            // with their byte tally on and the counts sent to scratch slots
+            const bool tal = mode == kBytesMode;
+            unsigned long long *acc = tal ? g.d_u64 + kU64Scratch : g.d_u64;
+            unsigned long long *acc_c = tal ? g.d_u64 + kU64Scratch + 1 : g.d_u64 + 3;
+            unsigned long long *acc_p = tal ? g.d_u64 + kU64Scratch + 2 : g.d_u64 + 4;
+            unsigned long long *acc_b = tal ? g.d_u64 + 2 : nullptr;
+            if (tal) CK(cudaMemsetAsync(fb.n, 0, 2 * sizeof(unsigned long long), g.stream));
+            const uint32_t wblocks =
+                std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(g_fused_walk_blocks), (pb - pa + kZW - 1) / kZW));
+            if (walk_ok && tal)
+                k_fused<kCountMode, true, true><<<wblocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
+                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, acc, acc_c, acc_p, acc_b);
+            else if (walk_ok)
+                k_fused<kCountMode, true><<<wblocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
+                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, acc, acc_c, acc_p, acc_b);
+            else
                 k_fused<kCountMode, false><<<blocks, kZW * 32, 0, g.stream>>>(view, dp, p, pa, pb, 1, split,
-                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64, g.d_u64 + 3, g.d_u64 + 4);
-            }
+                    g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, acc, acc_c, acc_p, acc_b);
             CK(cudaGetLastError());
             k_fused_scan<<<1, 1024, 0, g.stream>>>(fb);
             CK(cudaGetLastError());
             CK(cudaMemsetAsync(g.d_u32 + kSlotCursor, 0, sizeof(uint32_t), g.stream));
-            k_fused<kCountMode, false><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
-                view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, g.d_u64,
-                g.d_u64 + 3, g.d_u64 + 4);
+            if (tal)
+                k_fused<kCountMode, false, true><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
+                    view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, acc,
+                    acc_c, acc_p, acc_b);
+            else
+                k_fused<kCountMode, false><<<uint32_t(g_fused_blocks[kCountMode]), kZW * 32, 0, g.stream>>>(
+                    view, dp, p, pa, pb, 2, split, g.d_u32 + kSlotCursor, hp->fuse_scratch, hp->fuse_stride, fb, acc,
+                    acc_c, acc_p, acc_b);
             CK(cudaGetLastError());
             res.launches += 3;
         }
@@ -2084,6 +2147,9 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
     const bool fuse = counting && k >= 3 && hp->plan.lv[cl].fuse;
     if (fuse) stored = cl - 1;
     hp->stored = stored;
+    // before a fused count of levels p = cl - 1 and cl, the entries of
+    // level p - 1 record where their vertex sits in its list
+    hp->pos_lvl = (fuse && cl >= 3) ? cl - 2 : 0xffffffffu;
     if (!g.arena) {
         cudaError_t e = cudaMallocAsync(&g.arena, g.arena_bytes, g.stream);
         if (e != cudaSuccess) {
@@ -2146,7 +2212,7 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
 // Level 0 into L_0; returns |L_0|.
 int run_roots(DeviceGraph &g, Run &run, uint32_t shard, uint32_t nshards, uint32_t &n0) {
     CK(cudaMemsetAsync(g.d_u32, 0, sizeof(uint32_t) * kSlots, g.stream));
-    CK(cudaMemsetAsync(g.d_u64, 0, sizeof(unsigned long long) * 8, g.stream));
+    CK(cudaMemsetAsync(g.d_u64, 0, sizeof(unsigned long long) * kU64Slots, g.stream));
     n0 = 0;
     if (!g.n) return CUTS_OK;
     const uint32_t threads = 256;
@@ -2199,21 +2265,35 @@ int Run::write_rows(uint32_t nout) {
             rc = set_error(CUTS_ERR_CUDA, std::string("dump copy: ") + cudaGetErrorString(e));
             break;
         }
-        text.resize(size_t(nr) * k * 24 + 16);
-        char *w = text.data(), *end = text.data() + text.size();
-        for (uint32_t r = 0; r < nr; ++r) {
-            const uint32_t *row = h_rows + size_t(r) * k;
-            for (uint32_t j = 0; j < k; ++j) {
-                *w++ = '(';
-                w = std::to_chars(w, end, order[j]).ptr;
-                *w++ = ',';
-                w = std::to_chars(w, end, g.orig.empty() ? row[j] : g.orig[row[j]]).ptr;
-                *w++ = ')';
+        // text, formatted in parallel: each thread a contiguous block of
+        // rows into its own part of the buffer, written in row order
+        const size_t per_row = size_t(k) * 24 + 1;
+        text.resize(size_t(nr) * per_row + 16);
+        const int nth = std::max(1, std::min(omp_get_max_threads(), int((nr + 4095) / 4096)));
+        std::vector<size_t> used(size_t(nth), 0);
+        #pragma omp parallel for schedule(static, 1) num_threads(nth)
+        for (int t = 0; t < nth; ++t) {
+            const uint32_t r0 = uint32_t(uint64_t(nr) * t / nth), r1 = uint32_t(uint64_t(nr) * (t + 1) / nth);
+            char *const b0 = text.data() + size_t(r0) * per_row;
+            char *w = b0, *const end = text.data() + size_t(r1) * per_row;
+            for (uint32_t r = r0; r < r1; ++r) {
+                const uint32_t *row = h_rows + size_t(r) * k;
+                for (uint32_t j = 0; j < k; ++j) {
+                    *w++ = '(';
+                    w = std::to_chars(w, end, order[j]).ptr;
+                    *w++ = ',';
+                    w = std::to_chars(w, end, g.orig.empty() ? row[j] : g.orig[row[j]]).ptr;
+                    *w++ = ')';
+                }
+                *w++ = '\n';
             }
-            *w++ = '\n';
+            used[size_t(t)] = size_t(w - b0);
         }
-        if (std::fwrite(text.data(), 1, size_t(w - text.data()), dump_file) != size_t(w - text.data()))
-            rc = set_error(CUTS_ERR_IO, "short write to the dump file");
+        for (int t = 0; t < nth && rc == CUTS_OK; ++t) {
+            const char *b0 = text.data() + size_t(uint64_t(nr) * t / nth) * per_row;
+            if (std::fwrite(b0, 1, used[size_t(t)], dump_file) != used[size_t(t)])
+                rc = set_error(CUTS_ERR_IO, std::string("short write to the dump file: ") + std::strerror(errno));
+        }
         dumped += nr;
     }
     cudaFree(d_rows);
@@ -2291,7 +2371,9 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     return CUTS_OK;
 }
 
-int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines) {
+int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines, uint32_t shard,
+                uint32_t nshards) {
+    if (nshards == 0 || shard >= nshards) return set_error(CUTS_ERR_ARG, "bad shard");
     CK(cudaSetDevice(g.device));
     int rc = launch_geometry();
     if (rc) return rc;
@@ -2311,7 +2393,7 @@ int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *line
     run.dump_file = f;
     run.query = &q;
     uint32_t n0 = 0;
-    rc = run_roots(g, run, 0, 1, n0);
+    rc = run_roots(g, run, shard, nshards, n0);
     if (rc) return rc;
     if (n0 > 0) {
         rc = run_slices(run, n0, 1);

@@ -102,6 +102,8 @@ struct CountOptions {
 int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountResult &res);
 
 // Enumerates every embedding and writes ans.txt lines (util.cpp:53-74).
-int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines);
+// shard / nshards: only the roots u with u % nshards == shard (device ids).
+int device_dump(DeviceGraph &g, const Query &q, const char *path, uint64_t *lines, uint32_t shard = 0,
+                uint32_t nshards = 1);
 
 }  // namespace cuts

@@ -233,6 +233,15 @@ int cuts_count_sample(cuts_graph g, cuts_query q, uint32_t shard, uint32_t nshar
  * of lines in *count.  Line order is unspecified, as in the reference. */
 int cuts_dump(cuts_graph g, cuts_query q, const char *path, uint64_t *count);
 
+/* The matches of cuts_dump whose root (the data vertex matched at the first
+ * position of the order) is among the roots u with u % nshards == shard, in
+ * the engine's vertex numbering; the shards 0..nshards-1 together write every
+ * line of cuts_dump once.  Bounds one call's output on large graphs, where
+ * the reference holds every match in a 200 GB managed table
+ * (gpu_memory_allocation.cu:60-68) before writing ans.txt (util.cpp:53-74). */
+int cuts_dump_sharded(cuts_graph g, cuts_query q, uint32_t shard, uint32_t nshards, const char *path,
+                      uint64_t *count);
+
 /* Reference in-process API (host_funcs.h:21-25): load both files, make the
  * data graph resident, count, print "<data>,<query>,<ms>ms,<count>" and,
  * when write_to_disk != 0, write ans.txt in the working directory.

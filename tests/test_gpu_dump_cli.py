@@ -145,3 +145,22 @@ def test_dump_sets_equal_reference_binary(tmp_path):
             hsh.update((" ".join(str(x) for x in r) + "\n").encode())
         assert n == len(rows) == c["lines"], (key, c["query"])
         assert hsh.hexdigest() == c["sha256"] == c["oracle_sha256"], (key, c["query"])
+
+
+def test_sharded_dump_partitions_the_full_dump(tmp_path):
+    h = cb.HostGraph.chung_lu(3000, 12000, 2.2, 2.0, 60.0, seed=8)
+    g = h.upload(0)
+    for name in ["triangle", "house"]:
+        k, arcs = cb.named_query_arcs(name)
+        q = cb.Query.from_arcs(k, arcs)
+        full = str(tmp_path / f"{name}_full.txt")
+        n = g.dump(q, full)
+        rows = sorted(_parse_dump(full, q.order))
+        parts = []
+        for r in range(3):
+            path = str(tmp_path / f"{name}_{r}.txt")
+            nr = g.dump(q, path, r, 3)
+            pr = _parse_dump(path, q.order)
+            assert nr == len(pr) == g.count_sharded(q, r, 3).count
+            parts += pr
+        assert n == len(rows) and sorted(parts) == rows
