@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -415,11 +416,26 @@ void Batch::destroy() {
     h_ctr = nullptr;
 }
 
+// True when the level engine's plan for q counts its last levels fused or
+// orbit-folded (prepare() in engine.cu makes the same choice).
+static bool level_engine_pays(const Query &q, bool symmetric, uint32_t flags) {
+    Plan plan;
+    if (build_plan(q, symmetric, flags, plan)) return false;
+    const uint32_t k = q.k;
+    if (k < 3) return false;
+    if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && plan.lv[k - 1].ofold) return true;
+    const uint32_t cl = plan.lv[k - 2].fold ? k - 2 : k - 1;
+    return plan.lv[cl].fuse != 0 && !(flags & CUTS_FLAG_NO_FUSE);
+}
+
 int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_t flags_,
                   const BatchTuning &tune_) {
     g = &dg;
     flags = flags_;
     tune = tune_;
+    // CUTS_BATCH_ROUTE=0 keeps every query in the persistent launch (A/B)
+    const char *rt = std::getenv("CUTS_BATCH_ROUTE");
+    route_level = !(rt && rt[0] == '0');
     if (tune.grain == 0) tune.grain = 64;
     if (tune.tasks_per_grab == 0) tune.tasks_per_grab = 1;
     BCK(cudaSetDevice(g->device));
@@ -459,6 +475,11 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
                 B.jdir[t] = L.jdir[t];
             }
         }
+        // queries of 4+ vertices whose counted levels the level engine fuses
+        // (or, with symmetry breaking, orbit-folds) run there: its fused
+        // count, dense-core rows and hub split have no counterpart in the
+        // persistent kernel, which walks one candidate at a time
+        if (ok && q.k >= 4 && route_level && level_engine_pays(q, g->symmetric, flags)) ok = false;
         unsigned long long tasks = 0;
         if (ok) {
             b.k = q.k;
@@ -476,7 +497,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
                 index.push_back(i);
             }
         }
-        eligible[i] = ok ? 1 : (q.k >= 2 && n > 0 && q.k <= uint32_t(kBatchMaxK) ? 2 : 0);
+        eligible[i] = ok ? 1 : (b.root_cnt == 0 && b.k ? 2 : 0);
     }
     // eligible: 1 = in the launch, 2 = no root (count 0), 0 = counted by the level engine
     nb = uint32_t(hq.size());

@@ -46,6 +46,7 @@ struct Batch {
     uint32_t nb = 0;                 // queries in the launch
     std::vector<uint32_t> index;     // launch slot -> query
     std::vector<int> eligible;       // 1 in the launch, 2 no root, 0 level engine
+    bool route_level = true;         // fused / orbit-folded queries of 4+ vertices to the level engine
     std::vector<uint64_t> aut;       // count multiplier per query
     std::vector<unsigned long long> qbase_host;
     unsigned long long total_tasks = 0;

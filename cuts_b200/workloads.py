@@ -251,7 +251,20 @@ def run_batched(g: "cb.Graph", n: int = 4096, budget_ms: float = 60000.0, tune_s
     _log(f"batched: estimates {est_s:.1f} s, tuned {best} in {tune_s:.1f} s")
     counts, status, ms = b.run(budget_ms)
     fin = sum(1 for s in status if s == 0)
+    # the same finished queries one at a time through the level engine
+    # (count_budget, 10x the per-query share as a safety bound)
+    plain_ms, plain_done = 0.0, 0
+    for q, c, st in zip(qs, counts, status):
+        if st != 0:
+            continue
+        r, done = g.count_budget(q, 10 * query_budget_ms if query_budget_ms > 0 else 0.0, flags=flags)
+        if done:
+            assert r.count == c
+            plain_ms += r.ms
+            plain_done += 1
     return {"queries": n, "finished": fin, "launch_ms": ms, "queries_per_s": fin / (ms / 1e3),
+            "one_at_a_time": {"finished": plain_done, "ms": plain_ms,
+                              "queries_per_s": plain_done / max(plain_ms / 1e3, 1e-9)},
             "query_budget_ms": query_budget_ms, "launch_budget_ms": budget_ms,
             "tuned": list(best), "tune_s": tune_s, "estimate_s": est_s, "tasks": b.info()[0],
             "matches_finished": int(sum(c for c, s in zip(counts, status) if s == 0)),

@@ -199,3 +199,23 @@ def test_count_autotuner(name, flags):
     assert len(times) == 2 * 3 * 2 and best in times and times[best] == min(times.values())
     want = O.count(oracle_graph_from_host(h), O.Graph.from_arcs(k, arcs), q.order)[0]
     assert g.count(q, chunks=best[0], flags=flags).count == want
+
+
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK])
+def test_batch_routes_fused_queries_to_the_level_engine(pl, flags, monkeypatch):
+    """Queries of 4+ vertices whose count the level engine fuses (or
+    orbit-folds) leave the persistent launch; the counts are the same either
+    way and equal the oracle's."""
+    h, g, od = pl
+    names = ["4-clique+pendant", "house", "4-cycle", "triangle"]
+    qdefs = [cb.named_query_arcs(nm) for nm in names] + _queries(12, 4400)
+    qs = [cb.Query.from_arcs(k, a) for k, a in qdefs]
+    want = [O.count(od, O.Graph.from_arcs(k, a))[0] for k, a in qdefs]
+    routed = g.batch(qs, flags=flags)
+    monkeypatch.setenv("CUTS_BATCH_ROUTE", "0")
+    kept = g.batch(qs, flags=flags)
+    c1, s1, _ = routed.run()
+    c2, s2, _ = kept.run()
+    assert s1 == s2 == [0] * len(qs)
+    assert c1 == c2 == want
+    assert routed.info()[0] < kept.info()[0]  # fewer tasks in the launch
