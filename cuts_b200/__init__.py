@@ -34,6 +34,7 @@ FLAG_SYMMETRY_BREAK = 1
 FLAG_NO_CLOSED_FORM = 2
 FLAG_NO_FUSE = 4
 FLAG_NO_ORBIT_FOLD = 8
+FLAG_NO_PAIR_FOLD = 16
 ORDER_SCORE = 0
 ORDER_LEARNED = 1
 
@@ -332,12 +333,13 @@ class Query:
         """Per-level plan dicts (joins, sig, closed, fold, guar, gt, lt, fuse,
         ofold, qin, qout) and the count multiplier used."""
         k = self.k
-        out = np.zeros(11 * k, np.uint32)
+        out = np.zeros(12 * k, np.uint32)
         aut = C.c_uint64()
         _check(lib().cuts_query_plan_levels(self._h, int(data_symmetric), flags, _ptr(out, _u32p),
                                             C.byref(aut)))
-        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse", "ofold", "qin", "qout"]
-        return [dict(zip(keys, (int(x) for x in out[11 * i:11 * i + 11]))) for i in range(k)], aut.value
+        keys = ["joins", "sig", "closed", "fold", "guar", "gt", "lt", "fuse", "ofold", "qin", "qout",
+                "fold2"]
+        return [dict(zip(keys, (int(x) for x in out[12 * i:12 * i + 12]))) for i in range(k)], aut.value
 
     def automorphisms(self) -> int:
         a = C.c_uint64()

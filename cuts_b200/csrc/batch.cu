@@ -416,14 +416,16 @@ void Batch::destroy() {
     h_ctr = nullptr;
 }
 
-// True when the level engine's plan for q counts its last levels fused or
-// orbit-folded (prepare() in engine.cu makes the same choice).
+// True when the level engine's plan for q counts its last levels fused,
+// orbit-folded or as a pendant pair (prepare() in engine.cu makes the same
+// choices).
 static bool level_engine_pays(const Query &q, bool symmetric, uint32_t flags) {
     Plan plan;
     if (build_plan(q, symmetric, flags, plan)) return false;
     const uint32_t k = q.k;
     if (k < 3) return false;
     if ((flags & CUTS_FLAG_SYMMETRY_BREAK) && plan.lv[k - 1].ofold) return true;
+    if (k >= 4 && plan.lv[k - 3].fold2) return true;  // a pendant pair counted in closed form
     const uint32_t cl = plan.lv[k - 2].fold ? k - 2 : k - 1;
     return plan.lv[cl].fuse != 0 && !(flags & CUTS_FLAG_NO_FUSE);
 }
@@ -433,9 +435,11 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
     g = &dg;
     flags = flags_;
     tune = tune_;
-    // CUTS_BATCH_ROUTE=0 keeps every query in the persistent launch (A/B)
+    // CUTS_BATCH_ROUTE=0 keeps every query in the persistent launch, =2 sends
+    // every query of 4+ vertices to the level engine (A/B comparisons)
     const char *rt = std::getenv("CUTS_BATCH_ROUTE");
     route_level = !(rt && rt[0] == '0');
+    route_all = rt && rt[0] == '2';
     if (tune.grain == 0) tune.grain = 64;
     if (tune.tasks_per_grab == 0) tune.tasks_per_grab = 1;
     BCK(cudaSetDevice(g->device));
@@ -451,7 +455,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
     for (uint32_t i = 0; i < nq; ++i) {
         const Query &q = *qs[i];
         Plan plan;
-        rc = build_plan(q, g->symmetric, flags | CUTS_FLAG_NO_ORBIT_FOLD, plan);  // plain fold only
+        rc = build_plan(q, g->symmetric, flags | CUTS_FLAG_NO_ORBIT_FOLD | CUTS_FLAG_NO_PAIR_FOLD, plan);  // plain fold only
         if (rc) return rc;
         aut[i] = plan.aut;
         BQuery b;
@@ -479,7 +483,7 @@ int Batch::create(DeviceGraph &dg, const std::vector<const Query *> &qs, uint32_
         // (or, with symmetry breaking, orbit-folds) run there: its fused
         // count, dense-core rows and hub split have no counterpart in the
         // persistent kernel, which walks one candidate at a time
-        if (ok && q.k >= 4 && route_level && level_engine_pays(q, g->symmetric, flags)) ok = false;
+        if (ok && q.k >= 4 && route_level && (route_all || level_engine_pays(q, g->symmetric, flags))) ok = false;
         unsigned long long tasks = 0;
         if (ok) {
             b.k = q.k;
@@ -738,7 +742,7 @@ int count_noalloc(const uint32_t *info_out, const uint32_t *info_in, const uint3
         if (q.k > uint32_t(kBatchMaxK))
             return set_error(CUTS_ERR_LIMIT, "cuts_count_noalloc: query with more than 10 vertices");
         Plan plan;
-        int rc = build_plan(q, sym, flags | CUTS_FLAG_NO_ORBIT_FOLD, plan);  // plain fold only
+        int rc = build_plan(q, sym, flags | CUTS_FLAG_NO_ORBIT_FOLD | CUTS_FLAG_NO_PAIR_FOLD, plan);  // plain fold only
         if (rc) return rc;
         BQuery &b = table[i / kNoAllocPlansPerLaunch].q[i % kNoAllocPlansPerLaunch];
         std::memset(&b, 0, sizeof(b));

@@ -47,6 +47,7 @@ struct Batch {
     std::vector<uint32_t> index;     // launch slot -> query
     std::vector<int> eligible;       // 1 in the launch, 2 no root, 0 level engine
     bool route_level = true;         // fused / orbit-folded queries of 4+ vertices to the level engine
+    bool route_all = false;          // every query of 4+ vertices to the level engine
     std::vector<uint64_t> aut;       // count multiplier per query
     std::vector<unsigned long long> qbase_host;
     unsigned long long total_tasks = 0;

@@ -309,10 +309,10 @@ int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uin
         if (rc) return rc;
         for (uint32_t i = 0; i < q->q.k; ++i) {
             const LevelPlan &L = p.lv[i];
-            uint32_t *o = out + 11 * i;
+            uint32_t *o = out + 12 * i;
             o[0] = L.nj; o[1] = L.check_sig; o[2] = L.closed_form; o[3] = L.fold;
             o[4] = L.guar_mask; o[5] = L.gt_mask; o[6] = L.lt_mask; o[7] = L.fuse; o[8] = L.ofold;
-            o[9] = L.qin; o[10] = L.qout;
+            o[9] = L.qin; o[10] = L.qout; o[11] = L.fold2;
         }
         if (aut) *aut = p.aut;
         return CUTS_OK;

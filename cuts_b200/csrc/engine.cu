@@ -124,6 +124,61 @@ __device__ __forceinline__ uint32_t orbit_weight(const DevView &g, const LevelPl
     return w;
 }
 
+// Pendant pair (plan fold2 at level k-3; A = level k-2's plan, B = level
+// k-1's, both joining the same list): with m(j) the matched vertex of
+// position j <= k-3, the number of (t1, t2) with t1 in A's window of the
+// list, t2 in B's, both unmatched, t1 != t2, and -- kind 2 -- t2 above
+// (below) t1 on the same window.  O(log degree) per candidate.  Adds |A'|
+// (the level k-2 size) to lvl2.
+template <class M>
+__device__ uint64_t pendant_pairs(const DevView &g, const LevelPlan &A, const LevelPlan &B, uint32_t kind,
+                                  uint32_t lvl, bool loops, M m, unsigned long long &lvl2) {
+    const uint32_t pen = 1u << (lvl + 1);
+    uint32_t lo[2], hi[2], s0[2], e0[2], off[2], len[2], cnt[2], u[2];
+    for (int r = 0; r < 2; ++r) {
+        const LevelPlan &L = r ? B : A;
+        u[r] = m(L.jpos[0]);
+        const uint2 inf = L.jdir[0] ? g.in_info[u[r]] : g.out_info[u[r]];
+        off[r] = inf.x;
+        len[r] = inf.y;
+        lo[r] = 0;
+        hi[r] = kFullMask;
+        for (uint32_t msk = L.gt_mask & ~pen; msk; msk &= msk - 1) lo[r] = max(lo[r], m(__ffs(msk) - 1) + 1);
+        for (uint32_t msk = L.lt_mask & ~pen; msk; msk &= msk - 1) hi[r] = min(hi[r], m(__ffs(msk) - 1));
+        const uint32_t *l = g.adj + off[r];
+        const bool dir = L.jdir[0] != 0;
+        s0[r] = lo[r] ? lbound_own(g, dir, u[r], l, len[r], lo[r], loops) : 0;
+        e0[r] = hi[r] != kFullMask ? lbound_own(g, dir, u[r], l, len[r], hi[r], loops) : len[r];
+        if (e0[r] < s0[r]) e0[r] = s0[r];
+        const uint32_t guar = r ? B.guar_mask : A.guar1;
+        uint32_t sub = 0;
+        for (uint32_t j = 0; j <= lvl; ++j) {
+            const uint32_t mj = m(j);
+            if (mj >= lo[r] && mj < hi[r] && (((guar >> j) & 1u) || contains(l, len[r], mj))) ++sub;
+        }
+        cnt[r] = e0[r] - s0[r] - sub;
+    }
+    lvl2 += cnt[0];
+    if (kind == 2) return uint64_t(cnt[0]) * (cnt[0] - (cnt[0] ? 1 : 0)) / 2;
+    // |A'| |B'| - |A' n B'|
+    uint64_t both = 0;
+    const uint32_t wlo = max(lo[0], lo[1]), whi = min(hi[0], hi[1]);
+    if (wlo < whi) {
+        // one list: its entries in both windows form the window [wlo, whi)
+        const uint32_t a = max(s0[0], s0[1]), b = min(e0[0], e0[1]);
+        both = b > a ? b - a : 0;
+        // matched vertices lying in both windows and lists
+        for (uint32_t j = 0; j <= lvl; ++j) {
+            const uint32_t mj = m(j);
+            if (mj < wlo || mj >= whi) continue;
+            const bool in0 = ((A.guar1 >> j) & 1u) || contains(g.adj + off[0], len[0], mj);
+            const bool in1 = ((B.guar_mask >> j) & 1u) || contains(g.adj + off[1], len[1], mj);
+            if (in0 && in1) --both;
+        }
+    }
+    return uint64_t(cnt[0]) * cnt[1] - both;
+}
+
 enum Mode { kExpand = 0, kCountMode = 1, kBytesMode = 2 };
 
 // ---- level 0: signature scan (device_funcs.cu:267-279) ---------------
@@ -405,8 +460,8 @@ __global__ void __launch_bounds__(kFW * 32)
 k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t pa, uint32_t pb,
              uint32_t *__restrict__ cursor, uint32_t *__restrict__ out_n, uint32_t out_cap,
              uint32_t *__restrict__ err, unsigned long long *__restrict__ acc,
-             unsigned long long *__restrict__ acc2) {
-    __shared__ LevelPlan sL, sN;
+             unsigned long long *__restrict__ acc2, unsigned long long *__restrict__ acc3) {
+    __shared__ LevelPlan sL, sN, sN2;
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
     __shared__ uint32_t s_k, s_sym, s_stored;
@@ -424,6 +479,10 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
         const uint32_t *srcN = reinterpret_cast<const uint32_t *>(&rp->plan.lv[nl]);
         uint32_t *dN = reinterpret_cast<uint32_t *>(&sN);
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dN[i] = srcN[i];
+        const uint32_t nl2 = lvl + 2 < rp->plan.k ? lvl + 2 : nl;
+        const uint32_t *srcN2 = reinterpret_cast<const uint32_t *>(&rp->plan.lv[nl2]);
+        uint32_t *dN2 = reinterpret_cast<uint32_t *>(&sN2);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dN2[i] = srcN2[i];
         if (threadIdx.x < kMaxK) {
             s_vert[threadIdx.x] = rp->vert[threadIdx.x];
             s_par[threadIdx.x] = rp->par[threadIdx.x];
@@ -434,6 +493,9 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lanemask_lt = (1u << lane) - 1;
     const bool sym = s_sym != 0;
+    // pendant pair: this level (k-3) also counts levels k-2 and k-1
+    const uint32_t fold2 = MODE != kExpand ? sL.fold2 : 0u;
+    unsigned long long local3 = 0;
     const bool store_pos = MODE == kExpand && lvl == rp->pos_lvl;
     const bool need_ub = (MODE == kExpand && lvl + 1 < s_stored) || store_pos;
     uint32_t *out_v = MODE == kExpand ? rp->vert[lvl] : nullptr;
@@ -636,7 +698,14 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
                 }
             }
             if constexpr (MODE == kCountMode) {
-                if (fold) {
+                if (fold2) {
+                    if (ok) {
+                        const uint64_t p2 = pendant_pairs(g, sN, sN2, fold2, lvl, loops,
+                            [&](uint32_t j) { return j == lvl ? c : sm_m[warp][j][owner]; }, local3);
+                        local += p2;
+                        ++local2;
+                    }
+                } else if (fold) {
                     const uint32_t o_fbase = __shfl_sync(kFullMask, fbase, int(owner));
                     const uint32_t o_foff = __shfl_sync(kFullMask, f_off, int(owner));
                     const uint32_t o_fdeg = __shfl_sync(kFullMask, f_deg, int(owner));
@@ -680,9 +749,11 @@ k_level_flat(DevView g, const RunParams *__restrict__ rp, uint32_t lvl, uint32_t
         for (int s = 16; s; s >>= 1) {
             local += __shfl_xor_sync(kFullMask, local, s);
             local2 += __shfl_xor_sync(kFullMask, local2, s);
+            local3 += __shfl_xor_sync(kFullMask, local3, s);
         }
         if (lane == 0 && local) atomicAdd(acc, local);
         if (lane == 0 && local2 && acc2) atomicAdd(acc2, local2);
+        if (lane == 0 && local3 && acc3) atomicAdd(acc3, local3);
     }
 }
 
@@ -742,7 +813,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
     __shared__ uint32_t *s_vert[kMaxK];
     __shared__ uint32_t *s_par[kMaxK];
     __shared__ uint32_t wm[kZW][kMaxK];
-    __shared__ uint32_t joff[kZW][kMaxJ], jdeg[kZW][kMaxJ];
+    __shared__ uint32_t joff[kZW][kMaxJ], jdeg[kZW][kMaxJ], jver[kZW][kMaxJ];
     __shared__ uint32_t xoff[kZW][kMaxJ], xdeg[kZW][kMaxJ];
     // the pair walk's per-parent tables: S, and a hash table of the vertices
     // admissible as t (keys in buckets of 4, their index in S and term B)
@@ -1387,6 +1458,7 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                 md = inf.y;
                 joff[warp][lane] = mo;
                 jdeg[warp][lane] = md;
+                jver[warp][lane] = u;
             }
             uint32_t bd = md, bl = uint32_t(lane);
             #pragma unroll
@@ -1434,6 +1506,14 @@ k_fused(DevView g, const RunParams *__restrict__ rp, uint32_t p, uint32_t pa, ui
                         if (t == tmin) continue;
                         const uint32_t *lst = g.adj + joff[warp][t];
                         const uint32_t len2 = jdeg[warp][t];
+                        const uint32_t ut = jver[warp][t];
+                        if (g.core_bits && ut >= g.core0 && v >= g.core0) {
+                            // both in the dense core: one bit of ut's row
+                            const uint32_t bi = v - g.core0;
+                            const uint32_t w = __ldg(g.core_bits + size_t(ut - g.core0) * (kCore / 32) + (bi >> 5));
+                            if (!((w >> (bi & 31)) & 1u)) { ok = false; break; }
+                            continue;
+                        }
                         if (r < 2) {
                             const uint32_t pos = lbound_from(lst, len2, r == 0 ? gp0 : gp1, v);
                             if (r == 0) gp0 = pos; else gp1 = pos;
@@ -1714,6 +1794,7 @@ int launch_geometry() {
 enum : int { kSlotN0 = 0, kSlotErr = 1, kSlotNb = 2, kSlotOver = 3, kSlotOut = 8, kSlotCursor = 32, kSlots = 64 };
 constexpr int kU64Stamp = 5;  // d_u64 slot: device clock at the start of a budgeted run
 constexpr int kU64Scratch = 8;  // d_u64 slots 8..10: counts of the bytes pass (discarded)
+constexpr int kU64Pair = 6;     // d_u64 slot: level k-2 size of a pendant-pair count
 constexpr int kU64Slots = 16;
 
 }  // namespace
@@ -1908,13 +1989,13 @@ struct Run {
             unsigned long long *acc = mode == kBytesMode ? g.d_u64 + 2 : g.d_u64;
             if (mode == kExpand)
                 k_level_flat<kExpand><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, acc, nullptr);
+                    g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, acc, nullptr, nullptr);
             else if (mode == kCountMode)
                 k_level_flat<kCountMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, g.d_u64 + 3);
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, g.d_u64 + 3, g.d_u64 + kU64Pair);
             else
                 k_level_flat<kBytesMode><<<blocks, kFW * 32, 0, g.stream>>>(view, dp, lvl, pa, pb,
-                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, nullptr);
+                    g.d_u32 + kSlotCursor, out_n, 0, g.d_u32 + kSlotErr, acc, nullptr, nullptr);
         } else if (mode == kExpand)
             k_level<kExpand><<<blocks, kWarps * 32, 0, g.stream>>>(view, dp, lvl, pa, pb, grain,
                 g.d_u32 + kSlotCursor, out_n, uint32_t(cap), g.d_u32 + kSlotErr, g.d_u64);
@@ -2045,7 +2126,8 @@ struct Run {
         if (pb <= pa) return CUTS_OK;
         // the last level is counted; with a folded plan, level k-2 counts both;
         // with a fused plan, the counting kernel runs one level earlier
-        const uint32_t count_lvl = (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
+        const uint32_t count_lvl = (k >= 4 && hp->plan.lv[k - 3].fold2) ? k - 3
+                                   : (k >= 3 && hp->plan.lv[k - 2].fold) ? k - 2 : k - 1;
         if (!dump && k >= 3 && hp->plan.lv[count_lvl].fuse && lvl == count_lvl - 1)
             return launch_fused(bytes_mode ? kBytesMode : kCountMode, lvl, pa, pb);
         if (lvl == count_lvl && !dump) {
@@ -2133,6 +2215,19 @@ int prepare(DeviceGraph &g, const Query &q, uint32_t flags, uint32_t stored, Run
         }
     }
     hp->plan.data_loops = g.loops ? 1u : 0u;
+    if (k >= 4 && hp->plan.lv[k - 3].fold2) {
+        // the pendant pair is counted by the flattened kernel at level k-3;
+        // where that kernel does not run, plan without it
+        if (!counting || !g_use_flat || hp->plan.lv[k - 3].nj > uint32_t(kFJ)) {
+            rc = build_plan(q, g.symmetric, flags | CUTS_FLAG_NO_PAIR_FOLD |
+                                                (hp->plan.lv[k - 1].ofold ? 0u : CUTS_FLAG_NO_ORBIT_FOLD),
+                            hp->plan);
+            if (rc) return rc;
+            hp->plan.data_loops = g.loops ? 1u : 0u;
+        } else {
+            stored = k - 3;  // levels k-3.. are counted, not stored
+        }
+    }
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
         // the folded count runs in the flattened or the fused kernel only
         const bool fused_here = hp->plan.lv[k - 2].fuse != 0;
@@ -2340,6 +2435,11 @@ int device_count(DeviceGraph &g, const Query &q, const CountOptions &opt, CountR
     if (g.h_u32[kSlotOver]) return set_error(CUTS_ERR_BUDGET, "time budget exhausted");
     const uint64_t raw = k >= 2 ? uint64_t(g.h_u64[0]) : 0;
     res.level_sizes[k - 1] = k >= 2 ? raw : n0;
+    if (k >= 4 && hp->plan.lv[k - 3].fold2) {  // level k-3 counted both pendant levels
+        CK(cudaMemcpy(g.h_u64 + 3, g.d_u64 + 3, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost));
+        res.level_sizes[k - 3] = g.h_u64[3];
+        res.level_sizes[k - 2] = g.h_u64[kU64Pair];
+    }
     if (k >= 3 && hp->plan.lv[k - 2].fold) {
         CK(cudaMemcpy(g.h_u64 + 3, g.d_u64 + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         res.level_sizes[k - 2] = g.h_u64[3];

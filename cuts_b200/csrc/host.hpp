@@ -111,6 +111,12 @@ struct LevelPlan {
     uint32_t fuse_tp;         // index of c's join on position c-1
     uint32_t ofold;           // last level, orbit fold: positions x of the
                               // pendant's attachment orbit (0 = plain fold)
+    uint32_t fold2;           // level k-3: also counts levels k-2 and k-1,
+                              // two pendants on earlier positions (1: no
+                              // condition between them, 2: one list and
+                              // window, the second above / below the first)
+    uint32_t guar1;           // level k-2 of a pendant pair: positions whose
+                              // vertex the query guarantees in its list
     uint32_t oguar[kMaxK];    // orbit fold: positions j with m_j guaranteed
                               // in the list of m_x, per orbit position x
     uint8_t jpos[kMaxJ];      // joined position j

@@ -29,22 +29,25 @@ constexpr uint32_t kPad = 0xffffffffu;
 __device__ __forceinline__ uint32_t padded(uint32_t len) { return (len + 3u) & ~3u; }
 
 // Offsets monotone and within the arc count; every list strictly increasing
-// with ids below n.  flag |= 1 (offsets) or 2 (lists).
+// with ids below n.  flag |= 1 (offsets) or 2 (lists).  One warp per vertex,
+// its lanes across the list (coalesced; a hub's list no longer serialises
+// one thread).
 __global__ void k_validate(uint32_t n, uint64_t m, const uint64_t *__restrict__ off,
                            const uint32_t *__restrict__ adj, uint32_t *__restrict__ flag) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
         const uint64_t a = off[v], b = off[v + 1];
         if (b < a || b > m) {
-            atomicOr(flag, 1u);
+            if (lane == 0) atomicOr(flag, 1u);
             continue;
         }
-        for (uint64_t x = a; x < b; ++x) {
+        bool bad = false;
+        for (uint64_t x = a + lane; x < b; x += 32) {
             const uint32_t id = adj[x];
-            if (id >= n || (x > a && id <= adj[x - 1])) {
-                atomicOr(flag, 2u);
-                break;
-            }
+            if (id >= n || (x > a && id <= adj[x - 1])) bad = true;
         }
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, 2u);
     }
 }
 
@@ -249,8 +252,9 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     int rc = CUTS_OK;
     if (validate && n) {
         LCK(cudaMemsetAsync(d_flag, 0, sizeof(uint32_t), s));
-        k_validate<<<grid, 256, 0, s>>>(n, m, d_ooff, d_oadj, d_flag);
-        if (in_off) k_validate<<<grid, 256, 0, s>>>(n, m, d_ioff, d_iadj, d_flag);
+        const uint32_t vgrid = std::max<uint32_t>(1, std::min<uint32_t>((n + 7) / 8, 148u * 16));
+        k_validate<<<vgrid, 256, 0, s>>>(n, m, d_ooff, d_oadj, d_flag);
+        if (in_off) k_validate<<<vgrid, 256, 0, s>>>(n, m, d_ioff, d_iadj, d_flag);
         LCK(cudaGetLastError());
         if ((rc = read_flag())) return rc;
         if (h_flag & 1) return set_error(CUTS_ERR_ARG, "CSR offsets not monotone");
@@ -405,22 +409,35 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     auto odeg = [&](uint32_t v) { return uint32_t(out_off[v + 1] - out_off[v]); };
     auto ideg = [&](uint32_t v) { return symmetric ? odeg(v) : uint32_t(in_off[v + 1] - in_off[v]); };
     uint32_t maxd = 0;
-    for (uint32_t v = 0; v < n; ++v) maxd = std::max(maxd, std::max(odeg(v), ideg(v)));
+    #pragma omp parallel for reduction(max : maxd) schedule(static)
+    for (int64_t v = 0; v < int64_t(n); ++v) maxd = std::max(maxd, std::max(odeg(uint32_t(v)), ideg(uint32_t(v))));
     g.max_deg = maxd;
     g.h_out_deg.resize(n);
     g.h_in_deg.resize(n);
-    for (uint32_t d = 0; d < n; ++d) {
-        const uint32_t v = relabel ? orig[d] : d;
-        g.h_out_deg[d] = odeg(v);
-        g.h_in_deg[d] = ideg(v);
+    #pragma omp parallel for schedule(static)
+    for (int64_t d = 0; d < int64_t(n); ++d) {
+        const uint32_t v = relabel ? orig[size_t(d)] : uint32_t(d);
+        g.h_out_deg[size_t(d)] = odeg(v);
+        g.h_in_deg[size_t(d)] = ideg(v);
     }
     DegreeStats st;
     st.n = n;
     st.out_ge.assign(size_t(maxd) + 2, 0);
     st.in_ge.assign(size_t(maxd) + 2, 0);
-    for (uint32_t v = 0; v < n; ++v) {
-        st.out_ge[odeg(v)]++;
-        st.in_ge[ideg(v)]++;
+    // per-thread histograms while they are small; one pass otherwise
+    #pragma omp parallel if (maxd < (1u << 20))
+    {
+        std::vector<uint64_t> lo(size_t(maxd) + 2, 0), li(size_t(maxd) + 2, 0);
+        #pragma omp for schedule(static) nowait
+        for (int64_t v = 0; v < int64_t(n); ++v) {
+            lo[odeg(uint32_t(v))]++;
+            li[ideg(uint32_t(v))]++;
+        }
+        #pragma omp critical
+        for (size_t d = 0; d < lo.size(); ++d) {
+            st.out_ge[d] += lo[d];
+            st.in_ge[d] += li[d];
+        }
     }
     for (int64_t d = int64_t(maxd); d >= 0; --d) {
         st.out_ge[d] += st.out_ge[d + 1];

@@ -292,6 +292,9 @@ uint64_t automorphism_count(const Query &q) {
 // the level k-2 vertex must be implied by the query's arcs, so that the
 // per-candidate weight needs no list search.  Returns false (plan untouched)
 // when the query does not have that shape or the orbit is trivial.
+// The query vertex at order position jp.
+static inline uint32_t a_of(const Query &q, uint32_t jp) { return q.order[jp]; }
+
 static bool orbit_fold_plan(const Query &q, bool data_symmetric, Plan &plan) {
     const uint32_t k = q.k, c = k - 2;
     LevelPlan &F = plan.lv[k - 1];
@@ -428,13 +431,62 @@ int build_plan(const Query &q, bool data_symmetric, uint32_t flags, Plan &plan) 
         const uint32_t pen = 1u << (k - 2);
         if (F.jpos[0] != k - 2 && !(F.gt_mask & pen) && !(F.lt_mask & pen)) plan.lv[k - 2].fold = 1;
     }
+    // Pendant pair: the last two vertices are both pendants on earlier
+    // positions (each joins one list of a position below k-2, every query
+    // arc of theirs goes there, no self-loop -- so the joins imply their
+    // signatures) and both join the same list.  Their pairs (t1, t2) have a
+    // closed form per level k-3 candidate: with no condition between them,
+    // |A'| |B'| - |A' n B'| (A', B' the two windows of that list minus the
+    // matched vertices; A' n B' a window difference); with t2 above (or
+    // below) t1 on the same window, |A'| choose 2.  Level k-3 then counts
+    // both levels (plain orbit-free plans only).  Pendants on two different
+    // lists stay unfolded: |A' n B'| would be a serial intersection in one
+    // lane, over hub lists as long as the largest degree.
+    if (k >= 4 && !(flags & CUTS_FLAG_NO_PAIR_FOLD) && plan.lv[k - 1].closed_form && !plan.lv[k - 1].ofold) {
+        LevelPlan &L1 = plan.lv[k - 2];
+        const LevelPlan &L2 = plan.lv[k - 1];
+        const uint32_t p1 = k - 2, pen = 1u << p1;
+        const uint32_t v1 = q.order[p1];
+        bool ok = L1.nj == 1 && L1.jpos[0] < p1 && L2.jpos[0] == L1.jpos[0] &&
+                  L2.jdir[0] == L1.jdir[0] && !q.self_loop(v1) && q.sig_in.empty();
+        if (ok) {  // every arc of v1 goes to the vertex its list belongs to
+            const uint32_t a = q.order[L1.jpos[0]];
+            for (uint32_t w : q.out[v1]) ok = ok && w == a;
+            for (uint32_t w : q.in[v1]) ok = ok && w == a;
+        }
+        if (ok && !(L1.gt_mask & pen) && !(L1.lt_mask & pen)) {
+            const bool cond = ((L2.gt_mask | L2.lt_mask) & pen) != 0;
+            uint32_t kind = 0;
+            if (!cond) {
+                kind = 1;
+            } else if (((L2.gt_mask & pen) != 0) != ((L2.lt_mask & pen) != 0) &&
+                       L1.gt_mask == (L2.gt_mask & ~pen) &&
+                       L1.lt_mask == (L2.lt_mask & ~pen)) {
+                kind = 2;
+            }
+            if (kind) {
+                // matched vertices the query's arcs put in v1's list
+                const uint32_t jp = L1.jpos[0];
+                L1.guar1 = 0;
+                for (uint32_t j = 0; j < p1; ++j) {
+                    if (j == jp) continue;
+                    const uint32_t b = q.order[j];
+                    const bool fwd = L1.jdir[0] == 0 ? q.has_arc(a_of(q, jp), b) : q.has_arc(b, a_of(q, jp));
+                    const bool rev = L1.jdir[0] == 0 ? q.has_arc(b, a_of(q, jp)) : q.has_arc(a_of(q, jp), b);
+                    if (fwd || (data_symmetric && rev)) L1.guar1 |= 1u << j;
+                }
+                plan.lv[k - 3].fold2 = kind;
+                plan.lv[k - 2].fold = 0;
+            }
+        }
+    }
     // Fuse the counted level c with level p = c-1 when c's candidates are a
     // subset of p's: every list p joins is joined at c too, c also joins p's
     // own vertex, p's signature is no stricter than c's, and p's symmetry
     // window is no narrower than c's (p's conditions are among c's).  Then,
     // for one parent at level p-1, p's candidate set S serves every vertex s
     // chosen at p: c's candidates are the t in S that lie in s's list.
-    if (k >= 3 && !(flags & CUTS_FLAG_NO_FUSE)) {
+    if (k >= 3 && !(flags & CUTS_FLAG_NO_FUSE) && !(k >= 4 && plan.lv[k - 3].fold2)) {
         const uint32_t c = (plan.lv[k - 2].fold) ? k - 2 : k - 1;
         const uint32_t p = c - 1;
         LevelPlan &Lc = plan.lv[c];

@@ -41,6 +41,10 @@ extern "C" {
                                         whole query's symmetry even when the last
                                         vertex is a pendant whose removal leaves
                                         a more symmetric core */
+#define CUTS_FLAG_NO_PAIR_FOLD 16u   /* enumerate the second-to-last level even
+                                        when the last two vertices are pendants
+                                        on the same earlier vertex, whose pairs
+                                        have a closed form */
 
 /* order modes for cuts_plan */
 #define CUTS_ORDER_SCORE 0    /* greedy score order (score.cpp) */
@@ -159,11 +163,12 @@ int cuts_query_set_order(cuts_query q, const uint32_t *order);
 int cuts_query_prefix(cuts_query q, uint32_t j, cuts_query *out);
 
 /* The per-level plan the kernels run for the current order, for a data
- * graph that is symmetric or not and the given flags: 11 words per level,
+ * graph that is symmetric or not and the given flags: 12 words per level,
  * {joined lists, signature test, closed form, folded into the level before,
  * guaranteed-member mask, greater-than mask, less-than mask, fused with the
  * level before, orbit-fold positions, signature in-degree, signature
- * out-degree}.  Host only;
+ * out-degree, pendant-pair fold (1 independent pendants, 2 ordered pendants,
+ * both on one list: the level counts the last two levels' pairs)}.  Host only;
  * no reference counterpart (the reference derives joins per launch,
  * device_funcs.cu:103-127). */
 int cuts_query_plan_levels(cuts_query q, int data_symmetric, uint32_t flags, uint32_t *out,

@@ -33,27 +33,65 @@ def test_model_fits_training_levels(setup):
     assert L.prediction_error(model, X, y) < 1.0  # nats, teacher forced
 
 
-def test_learned_order_keeps_counts_and_gains(setup):
-    """Order never changes the count; the learned orders do less measured work
-    than the score orders over the held-out queries (the score order is the
-    fallback, so no query may get much worse)."""
+def _connected_orders(k, arcs):
+    nb = [set() for _ in range(k)]
+    for a, b in arcs:
+        if a != b:
+            nb[a].add(b)
+            nb[b].add(a)
+    out = []
+
+    def rec(o, used):
+        if len(o) == k:
+            out.append(list(o))
+            return
+        front = sorted({w for u in o for w in nb[u]} - used) if o else range(k)
+        for v in front:
+            o.append(v)
+            used.add(v)
+            rec(o, used)
+            o.pop()
+            used.discard(v)
+
+    rec([], set())
+    return out
+
+
+def test_learned_order_recovers_the_best_orders_gain(setup):
+    """Order never changes the count.  On the held-out queries (4 to 6
+    vertices), the best connected order of each query (found by counting
+    every one) does less work than the score order -- on this graph only
+    some 6-vertex queries leave room, the score order is already the best
+    order of every 4- and 5-vertex one; the learned order (the model's
+    search, score order kept unless it promises 1.5x less work) must
+    recover at least half of that reduction, on a log scale over the
+    queries -- so it fails when the model gains nothing."""
+    import math
     g, model, _, eval_q, _ = setup
-    w_score = w_learned = 0.0
+    lg_learned = lg_best = 0.0
     switched = 0
     for k, arcs in eval_q:
         q = cb.Query.from_arcs(k, arcs)
         rs = g.count(q, stats=True)
         ws = L.work(rs.level_sizes, k, L.joins_of(q))
+        best = ws
+        for o in _connected_orders(k, arcs):
+            q.set_order(o)
+            r = g.count(q, stats=True)
+            assert r.count == rs.count
+            best = min(best, L.work(r.level_sizes, k, L.joins_of(q)))
+        q = cb.Query.from_arcs(k, arcs)
         order, pw, sw = q.plan(g, cb.ORDER_LEARNED, model, margin=1.5)
         rl = g.count(q, stats=True)
         wl = L.work(rl.level_sizes, k, L.joins_of(q))
         assert rl.count == rs.count
-        w_score += ws
-        w_learned += wl
+        lg_learned += math.log(ws / max(wl, 1.0))
+        lg_best += math.log(ws / max(best, 1.0))
         switched += pw < sw
-    print(f"held-out work: score {w_score:.3e}, learned {w_learned:.3e}, "
-          f"gain {w_score / max(w_learned, 1):.2f}x, {switched}/{len(eval_q)} orders changed")
-    assert w_learned <= w_score
+    print(f"held-out work reduction (log): learned {lg_learned:.4f} of the best orders' {lg_best:.4f}, "
+          f"{switched} orders changed")
+    assert lg_best > 0
+    assert lg_learned >= 0.5 * lg_best
 
 
 def test_fallback_without_model(setup):

@@ -422,3 +422,52 @@ def test_sparse_graph(sparse5k, name, flags):
     cnt = _check(g, od, k, arcs, flags=flags, chunks=3, levels=not (flags & cb.FLAG_SYMMETRY_BREAK))
     if name.endswith("path") or name.endswith("star"):
         assert cnt > 0
+
+
+def _pendant_queries():
+    """Queries whose last two vertices are pendants on earlier ones: stars,
+    paths, a triangle with two tails on one / two vertices, random trees."""
+    qs = [cb.named_query_arcs(n) for n in ("3-star", "4-path", "5-path")]
+    sym = lambda es: [a for e in es for a in (e, e[::-1])]
+    qs.append((5, sym([(0, 1), (1, 2), (2, 0), (0, 3), (0, 4)])))          # two tails on one vertex
+    qs.append((5, sym([(0, 1), (1, 2), (2, 0), (0, 3), (1, 4)])))          # tails on two vertices
+    qs.append((6, sym([(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (2, 5)])))  # square with two tails
+    qs.append((5, sym([(0, 1), (0, 2), (0, 3), (0, 4)])))                  # 4-star
+    for s in range(6):
+        k = 5 + s % 3
+        qs.append((k, cb.random_query_arcs(k, 0.0, 9100 + s)))            # random trees
+    return qs
+
+
+@pytest.fixture(scope="module")
+def cl1k():
+    # power law with degree cap 20: the 7-vertex trees below have ~1e9 matches,
+    # which the oracle enumerates in a few seconds (on cl5k they take hours)
+    h = cb.HostGraph.chung_lu(1000, 2500, 2.1, 2.0, 20.0, seed=5)
+    return h, h.upload(0), oracle_graph_from_host(h)
+
+
+@pytest.mark.parametrize("i", range(13))
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK, cb.FLAG_NO_PAIR_FOLD])
+def test_pendant_pair_fold(cl1k, i, flags):
+    h, g, od = cl1k
+    k, arcs = _pendant_queries()[i]
+    q = cb.Query.from_arcs(k, arcs)
+    plan, _ = q.plan_levels(True, flags)
+    cnt = _check(g, od, k, arcs, flags=flags, chunks=2, levels=not (flags & cb.FLAG_SYMMETRY_BREAK))
+    assert cnt > 0
+    # stars and tails of two leaves on one vertex are folded; the others
+    # (pendants on two different vertices) check the unfolded plan
+    folded = i in (0, 3, 6, 9, 11) and not (flags & cb.FLAG_NO_PAIR_FOLD)
+    assert plan[k - 3]["fold2"] in ((1, 2) if folded else (0,))
+
+
+def test_pendant_pair_fold_directed():
+    n, src, dst = directed_er(1500, 14.0, seed=33)
+    oo, oa, io, ia, s, d = csr_from_arcs(n, src, dst)
+    g = cb.Graph.from_csr(n, oo, oa, io, ia)
+    od = O.Graph.from_arrays(n, s, d)
+    for arcs in ([(0, 1), (1, 2), (2, 0), (0, 3), (4, 0)], [(0, 1), (1, 2), (1, 3), (3, 4), (3, 5)],
+                 [(0, 1), (2, 1), (0, 3), (0, 4)]):
+        k = 1 + max(max(a) for a in arcs)
+        _check(g, od, k, arcs, chunks=1)

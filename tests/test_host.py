@@ -423,3 +423,27 @@ def test_query_prefix_keeps_the_first_levels_plan():
                 assert lv[i]["sig"] == 1 and lv[i]["closed"] == 0 and lv[i]["ofold"] == 0
     with pytest.raises(cb.CutsError):
         q.prefix(0)
+
+
+def test_pendant_pair_plan():
+    """The pendant-pair closed form is planned where the last two vertices
+    are pendants on the same earlier position: independent pendants (kind
+    1), or interchangeable ones ordered by symmetry breaking (kind 2); never
+    with CUTS_FLAG_NO_PAIR_FOLD, not when the two are adjacent, and not for
+    pendants on two different positions (a path's ends)."""
+    star = cb.Query.from_arcs(*cb.named_query_arcs("3-star"))
+    lv, aut = star.plan_levels(True, 0)
+    assert lv[1]["fold2"] == 1 and lv[2]["fold"] == 0 and aut == 1
+    lv, aut = star.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
+    assert lv[1]["fold2"] == 2 and aut == 6
+    lv, _ = star.plan_levels(True, cb.FLAG_NO_PAIR_FOLD)
+    assert all(x["fold2"] == 0 for x in lv)
+    path = cb.Query.from_arcs(*cb.named_query_arcs("4-path"))
+    assert all(x["fold2"] == 0 for x in path.plan_levels(True, 0)[0])
+    sym = lambda es: [a for e in es for a in (e, e[::-1])]
+    tails = cb.Query.from_arcs(5, sym([(0, 1), (1, 2), (2, 0), (0, 3), (0, 4)]))  # two tails on one vertex
+    assert tails.plan_levels(True, 0)[0][2]["fold2"] == 1
+    assert tails.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)[0][2]["fold2"] == 2
+    # a triangle's last two vertices are adjacent: no pendant pair
+    tri = cb.Query.from_arcs(*cb.named_query_arcs("4-clique+pendant"))
+    assert all(x["fold2"] == 0 for x in tri.plan_levels(True, 0)[0])
