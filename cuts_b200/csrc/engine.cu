@@ -1867,13 +1867,16 @@ int device_graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *o
 void device_graph_free(DeviceGraph *g) {
     if (!g) return;
     cudaSetDevice(g->device);
-    if (g->arena && g->stream) cudaFreeAsync(g->arena, g->stream);  // back to the pool
-    if (g->stream) cudaStreamSynchronize(g->stream);
-    if (g->in_info && g->in_info != g->out_info) cudaFree(g->in_info);
-    cudaFree(g->out_info);
-    cudaFree(g->adj);
-    cudaFree(g->bwd_out);
-    cudaFree(g->core_bits);
+    if (g->stream) {
+        // the arena and the layout's arrays go back to the device's pool,
+        // after the work queued on the graph's stream
+        if (g->in_info && g->in_info != g->out_info) cudaFreeAsync(g->in_info, g->stream);
+        for (void *p : {static_cast<void *>(g->arena), static_cast<void *>(g->out_info),
+                        static_cast<void *>(g->adj), static_cast<void *>(g->bwd_out),
+                        static_cast<void *>(g->core_bits)})
+            if (p) cudaFreeAsync(p, g->stream);
+        cudaStreamSynchronize(g->stream);
+    }
     cudaFree(g->d_u32);
     cudaFree(g->d_u64);
     cudaFree(g->d_plan);

@@ -59,22 +59,47 @@ __global__ void k_differ(uint64_t cnt, const T *__restrict__ a, const T *__restr
         if (a[i] != b[i]) atomicOr(flag, 1u);
 }
 
-// Every arc u -> v has its reverse: one warp per vertex u, a binary search
-// for u in v's (validated, sorted) list per arc.
+// Every arc u -> v has its reverse.  Order the vertices by (degree, id).
+// With no repeated arc (the lists were checked strictly increasing),
+// reversal maps the arcs that go down in that order one-to-one into the
+// arcs that go up, once every down arc's reverse is found; the two sets then
+// have equal sizes exactly when every up arc's reverse exists too.  So only
+// a down arc u -> v is searched for, as u in v's list -- the shorter of the
+// two: a hub's list is never searched -- and the arcs going up and down are
+// counted into updown[0] / updown[1] (a self-loop is its own reverse).  One
+// warp per vertex u.
 __global__ void k_symmetric(uint32_t n, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
-                            uint32_t *__restrict__ flag) {
+                            uint32_t *__restrict__ flag, unsigned long long *__restrict__ updown) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long up = 0, down = 0;
     for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
-        for (uint64_t x = off[u] + lane; x < off[u + 1]; x += 32) {
+        const uint64_t a = off[u], b = off[u + 1];
+        const uint64_t du = b - a;
+        for (uint64_t x = a + lane; x < b; x += 32) {
             const uint32_t v = adj[x];
-            uint64_t lo = off[v], hi = off[v + 1];
+            if (v == u) continue;
+            const uint64_t lo0 = off[v], hi0 = off[v + 1], dv = hi0 - lo0;
+            if (!(dv < du || (dv == du && v < u))) {
+                ++up;
+                continue;
+            }
+            ++down;
+            uint64_t lo = lo0, hi = hi0;
             while (lo < hi) {
                 const uint64_t mid = (lo + hi) >> 1;
                 if (adj[mid] < u) lo = mid + 1; else hi = mid;
             }
-            if (lo == off[v + 1] || adj[lo] != u) atomicOr(flag, 1u);
+            if (lo == hi0 || adj[lo] != u) atomicOr(flag, 1u);
         }
+    }
+    for (int sh = 16; sh; sh >>= 1) {
+        up += __shfl_xor_sync(0xffffffffu, up, sh);
+        down += __shfl_xor_sync(0xffffffffu, down, sh);
+    }
+    if (lane == 0 && (up | down)) {
+        atomicAdd(updown, up);
+        atomicAdd(updown + 1, down);
     }
 }
 
@@ -262,6 +287,7 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     }
     // symmetry: given, compared with the in-lists, or checked arc by arc
     bool symmetric = sym_hint == 1;
+    unsigned long long *d_updown = nullptr, h_updown[2] = {0, 0};
     if (sym_hint < 0) {
         LCK(cudaMemsetAsync(d_flag, 0, sizeof(uint32_t), s));
         if (in_off) {
@@ -269,12 +295,15 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
             const uint32_t g2 = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>((m + 255) / 256, 148u * 16)));
             if (m) k_differ<uint32_t><<<g2, 256, 0, s>>>(m, d_oadj, d_iadj, d_flag);
         } else if (n) {
+            LCK(sc.get(&d_updown, 2));
+            LCK(cudaMemsetAsync(d_updown, 0, 2 * sizeof(unsigned long long), s));
             k_symmetric<<<std::max<uint32_t>(1, std::min<uint32_t>((n + 7) / 8, 148u * 16)), 256, 0, s>>>(
-                n, d_ooff, d_oadj, d_flag);
+                n, d_ooff, d_oadj, d_flag, d_updown);
+            LCK(cudaMemcpyAsync(h_updown, d_updown, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         }
         LCK(cudaGetLastError());
         if ((rc = read_flag())) return rc;
-        symmetric = h_flag == 0;
+        symmetric = h_flag == 0 && h_updown[0] == h_updown[1];
         if (!in_off && !symmetric)
             return set_error(CUTS_ERR_ARG, "in-lists omitted but the graph is not symmetric");
     }
@@ -286,7 +315,8 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     uint64_t pre_words = 0;
     for (int dir = 0; dir < (symmetric ? 1 : 2); ++dir) {
         const uint64_t *off = dir ? in_off : out_off;
-        for (uint32_t v = 0; v < n; ++v) pre_words += (off[v + 1] - off[v] + 3) & ~uint64_t(3);
+        #pragma omp parallel for reduction(+ : pre_words) schedule(static)
+        for (int64_t v = 0; v < int64_t(n); ++v) pre_words += (off[v + 1] - off[v] + 3) & ~uint64_t(3);
     }
     const char *nr = std::getenv("CUTS_NO_RELABEL");
     const bool relabel = !(nr && nr[0] == '1') && n > 1 && pre_words < (uint64_t(1) << 31);
@@ -335,10 +365,12 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     if (total >= (uint64_t(1) << 32)) return set_error(CUTS_ERR_LIMIT, "padded adjacency exceeds 2^32 words");
 
     // device-resident arrays of the graph (owned by g from here on)
-    LCK(cudaMalloc(&g.out_info, sizeof(uint2) * std::max<uint32_t>(n, 1)));
+    // the graph's own arrays come from the device's default pool too (freed
+    // with cudaFreeAsync by device_graph_free), so a rebuilt graph reuses them
+    LCK(cudaMallocAsync(reinterpret_cast<void **>(&g.out_info), sizeof(uint2) * std::max<uint32_t>(n, 1), s));
     if (symmetric) g.in_info = g.out_info;
-    else LCK(cudaMalloc(&g.in_info, sizeof(uint2) * std::max<uint32_t>(n, 1)));
-    LCK(cudaMalloc(&g.adj, sizeof(uint32_t) * total));
+    else LCK(cudaMallocAsync(reinterpret_cast<void **>(&g.in_info), sizeof(uint2) * std::max<uint32_t>(n, 1), s));
+    LCK(cudaMallocAsync(reinterpret_cast<void **>(&g.adj), sizeof(uint32_t) * total, s));
     LCK(cudaMemsetAsync(g.adj, 0xff, sizeof(uint32_t) * total, s));
     uint32_t *seg_b = nullptr, *seg_e = nullptr, *fill = g.adj;
     if (relabel) {
@@ -377,7 +409,7 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     g.loops = h_flag != 0;
     // per-vertex counts of list entries below the vertex (windows that start
     // or end at a list's own vertex need no search)
-    LCK(cudaMalloc(&g.bwd_out, sizeof(uint32_t) * std::max<uint32_t>(n, 1) * (symmetric ? 1 : 2)));
+    LCK(cudaMallocAsync(reinterpret_cast<void **>(&g.bwd_out), sizeof(uint32_t) * std::max<uint32_t>(n, 1) * (symmetric ? 1 : 2), s));
     g.bwd_in = symmetric ? g.bwd_out : g.bwd_out + n;
     if (n) {
         k_bwd<<<grid, 256, 0, s>>>(n, g.out_info, g.adj, g.bwd_out);
@@ -389,7 +421,7 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
         // ranking), as an adjacency bitmap
         g.core0 = n > kCore ? n - kCore : 0;
         const size_t words = size_t(kCore) * (kCore / 32);
-        LCK(cudaMalloc(&g.core_bits, words * sizeof(uint32_t)));
+        LCK(cudaMallocAsync(reinterpret_cast<void **>(&g.core_bits), words * sizeof(uint32_t), s));
         LCK(cudaMemsetAsync(g.core_bits, 0, words * sizeof(uint32_t), s));
         k_core_bits<<<(kCore * 32 + 255) / 256, 256, 0, s>>>(n, g.core0, g.out_info, g.adj, g.core_bits);
         LCK(cudaGetLastError());

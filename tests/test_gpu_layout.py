@@ -54,6 +54,52 @@ def test_from_csr_rejects_invalid_input():
     assert g.count(cb.Query.from_arcs(*cb.named_query_arcs("5-cycle"))).count == 10
 
 
+def _drop_arc(oo, oa, u, v):
+    """The CSR without the arc u -> v."""
+    x = int(oo[u]) + int(np.searchsorted(oa[oo[u]:oo[u + 1]], v))
+    assert oa[x] == v
+    oo2 = oo.copy()
+    oo2[u + 1:] -= 1
+    return oo2, np.delete(oa, x)
+
+
+def test_symmetry_check_finds_every_missing_reverse():
+    """The symmetry check searches only the arcs that go down in (degree,
+    id) order and compares the numbers of arcs going up and down: a missing
+    reverse is found on either side, from a hub or from a leaf."""
+    # star 0-1, 0-2 plus the arc 3 -> 0 alone (an up arc: leaf to hub), and
+    # 0 -> 3 alone (a down arc: hub to leaf)
+    for extra in ([(3, 0)], [(0, 3)]):
+        src = np.array([0, 1, 0, 2] + [a for a, b in extra], np.uint32)
+        dst = np.array([1, 0, 2, 0] + [b for a, b in extra], np.uint32)
+        oo, oa, _, _, _, _ = csr_from_arcs(4, src, dst)
+        with pytest.raises(cb.CutsError, match="not symmetric"):
+            cb.Graph.from_csr(4, oo, oa)
+    # a power-law graph, self-loops added: symmetric; without one arc (hub
+    # to leaf, leaf to hub, equal degrees): not
+    h = cb.HostGraph.chung_lu(3000, 9000, 2.1, 2.0, 200.0, seed=12)
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(h.n, dtype=np.uint32), np.diff(oo).astype(np.int64))
+    loops = np.arange(0, h.n, 7, dtype=np.uint32)
+    lo, la, _, _, _, _ = csr_from_arcs(h.n, np.concatenate([src, loops]), np.concatenate([oa, loops]))
+    assert cb.Graph.from_csr(h.n, lo, la).info()[2] is True
+    deg = np.diff(oo)
+    hub = int(np.argmax(deg))
+    leaf = int(oa[oo[hub]:oo[hub + 1]][np.argmin(deg[oa[oo[hub]:oo[hub + 1]]])])
+    pairs = [(hub, leaf), (leaf, hub)]
+    for u in range(h.n):  # an arc between two vertices of equal degree
+        vs = oa[oo[u]:oo[u + 1]]
+        same = vs[deg[vs] == deg[u]]
+        if len(same):
+            pairs += [(u, int(same[0])), (int(same[0]), u)]
+            break
+    assert len(pairs) == 4
+    for u, v in pairs:
+        oo2, oa2 = _drop_arc(oo, oa, u, v)
+        with pytest.raises(cb.CutsError, match="not symmetric"):
+            cb.Graph.from_csr(h.n, oo2, oa2)
+
+
 def test_host_and_csr_paths_agree():
     h = cb.HostGraph.chung_lu(5000, 20000, 2.1, 2.0, 100.0, seed=5)
     oo, oa, _, _ = h.csr()
