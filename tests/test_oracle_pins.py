@@ -81,7 +81,7 @@ def test_reference_query_fixtures_live():
         assert eq.joins() == (P, C)
 
 
-def test_survey_examples():
+def test_four_cycle_order_and_joins():
     # symmetric 4-cycle -> order 0 1 2 3 with P = C = {0, 2} at the last level
     k, arcs = cb.named_query_arcs("4-cycle")
     order, P, C = O.order(O.Graph.from_arcs(k, arcs))
