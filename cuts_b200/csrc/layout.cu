@@ -456,8 +456,9 @@ int device_layout(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj, 
     st.n = n;
     st.out_ge.assign(size_t(maxd) + 2, 0);
     st.in_ge.assign(size_t(maxd) + 2, 0);
-    // per-thread histograms while they are small; one pass otherwise
-    #pragma omp parallel if (maxd < (1u << 20))
+    // per-thread histograms while they are small (two of 8 B x (maxd + 2)
+    // per thread: 1 MB at the bound); one pass otherwise
+    #pragma omp parallel if (maxd < (1u << 16))
     {
         std::vector<uint64_t> lo(size_t(maxd) + 2, 0), li(size_t(maxd) + 2, 0);
         #pragma omp for schedule(static) nowait
