@@ -59,6 +59,65 @@ def test_loader_matches_oracle(tmp_path, name):
         assert np.array_equal(io, pi) and np.array_equal(ia, pia)
 
 
+REF_LOADER_JSON = os.path.join(os.path.dirname(__file__), "golden", "ref_loader.json")
+REF_LOAD = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                        "ref_load")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_loader_matches_reference_loader(tmp_path, name):
+    """This loader builds the CSR that the reference's own loader builds
+    (file_reader, util.cpp:19-52; Graph(1, path), graph.cpp:18-61) on every
+    edge case: vertex and arc counts, out-lists and in-lists.  Fixtures from
+    the reference loader compiled from its sources
+    (tests/golden/make_ref_loader.py); the binary is run live as well where
+    it has been built."""
+    import json
+    with open(REF_LOADER_JSON) as f:
+        want = json.load(f)[name]
+    p = str(tmp_path / "g.txt")
+    with open(p, "w", newline="") as f:
+        f.write(CASES[name])
+    if os.path.exists(REF_LOAD):
+        from tests.golden.make_ref_loader import run_ref_load
+        assert run_ref_load(p) == want
+    h = cb.HostGraph.load(p)
+    n, arcs, sym, _ = h.info()
+    assert (n, arcs) == (want["V"], want["E"])
+    oo, oa, io, ia = h.csr()
+    assert oo.tolist() == want["out_off"] and oa.tolist() == want["out_adj"]
+    if sym:  # one CSR kept: the reference's in-lists are the same lists
+        assert want["in_off"] == want["out_off"] and want["in_adj"] == want["out_adj"]
+    else:
+        assert io.tolist() == want["in_off"] and ia.tolist() == want["in_adj"]
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LOAD), reason="reference loader not built here")
+def test_loader_matches_reference_loader_on_random_files(tmp_path):
+    """Seeded random files -- directed arcs with repeats and self-loops in
+    random line order, CRLF line ends on some lines -- loaded by the
+    reference's loader and by this one: the same CSR."""
+    from tests.golden.make_ref_loader import run_ref_load
+    rng = np.random.default_rng(5)
+    for n, m in ((50, 400), (3000, 40000)):
+        src = rng.integers(0, n, m)
+        dst = rng.integers(0, n, m)
+        src = np.concatenate([src, src[: m // 10]])  # repeated arcs
+        dst = np.concatenate([dst, dst[: m // 10]])
+        perm = rng.permutation(len(src))
+        ends = rng.choice(["\n", "\r\n"], len(src))
+        p = str(tmp_path / f"r{n}.txt")
+        with open(p, "w", newline="") as f:
+            f.write(f"{n}\n" + "".join(f"{src[i]}\t{dst[i]}{ends[i]}" for i in perm))
+        want = run_ref_load(p)
+        h = cb.HostGraph.load(p)
+        n2, arcs, sym, _ = h.info()
+        assert (n2, arcs) == (want["V"], want["E"])
+        oo, oa, io, ia = h.csr()
+        assert oo.tolist() == want["out_off"] and oa.tolist() == want["out_adj"]
+        assert not sym and io.tolist() == want["in_off"] and ia.tolist() == want["in_adj"]
+
+
 @pytest.mark.parametrize("text,code", [
     ("", cb.ERR_PARSE),
     ("x\n0\t1\n", cb.ERR_PARSE),
