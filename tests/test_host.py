@@ -450,6 +450,105 @@ def _orbit_case(name, directed, k, arcs, n, src, dst):
     assert all(l["ofold"] == 0 for l in lvn)
 
 
+def _pair_queries():
+    """Queries whose last two vertices may be pendants on one vertex: stars,
+    tails on one or two vertices, a path, random trees."""
+    sym = lambda es: [a for e in es for a in (e, e[::-1])]
+    qs = [cb.named_query_arcs(x) for x in ("3-star", "4-path")]
+    qs.append((5, sym([(0, 1), (1, 2), (2, 0), (0, 3), (0, 4)])))  # two tails on one vertex
+    qs.append((5, sym([(0, 1), (1, 2), (2, 0), (0, 3), (1, 4)])))  # tails on two vertices
+    qs.append((5, sym([(0, 1), (0, 2), (0, 3), (0, 4)])))          # 4-star
+    qs += [(5 + s % 2, cb.random_query_arcs(5 + s % 2, 0.0, 9100 + s)) for s in range(4)]
+    return qs
+
+
+def _brute_pair_total(q, qarcs, lv, aut, n, out_adj, in_adj):
+    """aut x the pendant-pair closed form as the counting kernel evaluates
+    it: every embedding of the first k - 2 positions that satisfies the
+    plan's masks and signatures, times |A'| |B'| - |A' n B'| (kind 1) or
+    C(|A'|, 2) (kind 2), A' and B' the two pendants' windows of their list
+    minus the matched vertices (no signature test for the pendants: the
+    plan holds that the joins imply it)."""
+    k = q.k
+    order = q.order
+    arcs = set(qarcs)
+    kind = lv[k - 3]["fold2"]
+    m = []
+    total = 0
+
+    def fits(i, v):
+        if v in m:
+            return False
+        if lv[i]["sig"] and (len(in_adj[v]) < lv[i]["qin"] or len(out_adj[v]) < lv[i]["qout"]):
+            return False
+        for j in range(i):
+            if (order[i], order[j]) in arcs and m[j] not in out_adj[v]:
+                return False
+            if (order[j], order[i]) in arcs and v not in out_adj[m[j]]:
+                return False
+            if ((lv[i]["gt"] >> j) & 1) and not v > m[j]:
+                return False
+            if ((lv[i]["lt"] >> j) & 1) and not v < m[j]:
+                return False
+        return True
+
+    def window(pos):
+        x = order[pos]
+        a = [j for j in range(k - 2) if (order[j], x) in arcs or (x, order[j]) in arcs]
+        assert len(a) == 1
+        j = a[0]
+        lst = out_adj[m[j]] if (order[j], x) in arcs else in_adj[m[j]]
+        lo, hi = 0, 1 << 40
+        for jj in range(k - 2):  # conditions on earlier positions (the pen bit excluded)
+            if (lv[pos]["gt"] >> jj) & 1:
+                lo = max(lo, m[jj] + 1)
+            if (lv[pos]["lt"] >> jj) & 1:
+                hi = min(hi, m[jj])
+        return {t for t in lst if lo <= t < hi} - set(m)
+
+    def dfs(i):
+        nonlocal total
+        if i == k - 2:
+            A, B = window(k - 2), window(k - 1)
+            total += len(A) * (len(A) - 1) // 2 if kind == 2 else len(A) * len(B) - len(A & B)
+            return
+        for v in range(n):
+            if fits(i, v):
+                m.append(v)
+                dfs(i + 1)
+                m.pop()
+
+    dfs(0)
+    return total * aut
+
+
+@pytest.mark.parametrize("directed", [False, True])
+@pytest.mark.parametrize("flags", [0, cb.FLAG_SYMMETRY_BREAK])
+def test_pendant_pair_plan_is_exact(directed, flags):
+    """Where the plan folds a pendant pair, its closed form over the plan's
+    own masks equals the oracle's count; every fold is on one list."""
+    folded = 0
+    for qi, (k, arcs) in enumerate(_pair_queries()):
+        if directed:
+            arcs = [(a, b) for a, b in arcs if a < b]
+        for n, src, dst in _orbit_graphs(directed, k):
+            out_adj = [set() for _ in range(n)]
+            in_adj = [set() for _ in range(n)]
+            for u, v in zip(src, dst):
+                out_adj[u].add(v)
+                in_adj[v].add(u)
+            sym = all(u in out_adj[v] for u in range(n) for v in out_adj[u])
+            q = cb.Query.from_arcs(k, arcs)
+            lv, aut = q.plan_levels(sym, flags)
+            if not lv[k - 3]["fold2"]:
+                continue
+            folded += 1
+            og = O.Graph.from_arrays(n, np.array(src, np.uint32), np.array(dst, np.uint32))
+            want = O.count(og, O.Graph.from_arcs(k, arcs), q.order)[0]
+            assert _brute_pair_total(q, arcs, lv, aut, n, out_adj, in_adj) == want, (qi, directed, flags)
+    assert folded >= 6
+
+
 def test_orbit_fold_plan_shape():
     q = cb.Query.from_arcs(*cb.named_query_arcs("4-clique+pendant"))
     lv, aut = q.plan_levels(True, cb.FLAG_SYMMETRY_BREAK)
