@@ -16,7 +16,11 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "host.hpp"
 
@@ -87,18 +91,32 @@ static void build_one_csr(uint32_t n, const std::vector<uint32_t> &key,
         std::memcpy(adj.data() + off[v], tmp.data() + raw[v], len[v + 1] * sizeof(uint32_t));
 }
 
+// Every arc has its reverse (lists strictly increasing).  Vertices ordered
+// by (degree, id): reversal maps the arcs going down one-to-one into the
+// arcs going up once each down arc's reverse is found, so only down arcs are
+// searched -- in the lower vertex's, shorter, list -- and the two kinds are
+// counted: equal counts mean every up arc's reverse exists too.
 static bool check_symmetric(const HostGraph &g) {
     std::atomic<bool> ok{true};
-    #pragma omp parallel for schedule(dynamic, 1024)
+    uint64_t up = 0, down = 0;
+    #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : up, down)
     for (int64_t u = 0; u < int64_t(g.n); ++u) {
         if (!ok.load(std::memory_order_relaxed)) continue;
+        const uint64_t du = g.out_off[u + 1] - g.out_off[u];
         for (uint64_t a = g.out_off[u]; a < g.out_off[u + 1]; ++a) {
-            uint32_t v = g.out_adj[a];
+            const uint32_t v = g.out_adj[a];
+            if (v == uint32_t(u)) continue;
+            const uint64_t dv = g.out_off[v + 1] - g.out_off[v];
+            if (!(dv < du || (dv == du && v < uint32_t(u)))) {
+                ++up;
+                continue;
+            }
+            ++down;
             const uint32_t *b = g.out_adj.data() + g.out_off[v], *e = g.out_adj.data() + g.out_off[v + 1];
             if (!std::binary_search(b, e, uint32_t(u))) { ok.store(false); break; }
         }
     }
-    return ok.load();
+    return ok.load() && up == down;
 }
 
 int graph_from_arcs(uint32_t n, std::vector<uint32_t> &src, std::vector<uint32_t> &dst,
@@ -164,19 +182,39 @@ int graph_from_csr(uint32_t n, const uint64_t *out_off, const uint32_t *out_adj,
     return CUTS_OK;
 }
 
-int load_graph_text(const std::string &path, HostGraph &g) {
-    FILE *f = std::fopen(path.c_str(), "rb");
-    if (!f) return set_error(CUTS_ERR_IO, "load graph file failed: " + path);
-    std::fseek(f, 0, SEEK_END);
-    long sz = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    std::vector<char> buf(size_t(sz > 0 ? sz : 0) + 1);
-    if (sz > 0 && std::fread(buf.data(), 1, size_t(sz), f) != size_t(sz)) {
-        std::fclose(f);
-        return set_error(CUTS_ERR_IO, "short read: " + path);
+// The file's bytes, mapped read-only (the page cache, no copy); unmapped on
+// destruction.
+struct MappedFile {
+    const char *data = nullptr;
+    size_t size = 0;
+    ~MappedFile() {
+        if (data) munmap(const_cast<char *>(data), size);
     }
-    std::fclose(f);
-    const char *p = buf.data(), *end = buf.data() + (sz > 0 ? sz : 0);
+};
+
+int load_graph_text(const std::string &path, HostGraph &g) {
+    MappedFile mf;
+    {
+        const int fd = open(path.c_str(), O_RDONLY);
+        if (fd < 0) return set_error(CUTS_ERR_IO, "load graph file failed: " + path);
+        struct stat st;
+        if (fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) {
+            close(fd);
+            return set_error(CUTS_ERR_IO, "load graph file failed (not a regular file): " + path);
+        }
+        mf.size = size_t(st.st_size);
+        if (mf.size) {
+            void *m = mmap(nullptr, mf.size, PROT_READ, MAP_PRIVATE | MAP_POPULATE, fd, 0);
+            if (m == MAP_FAILED) {
+                close(fd);
+                return set_error(CUTS_ERR_IO, "cannot map " + path);
+            }
+            mf.data = static_cast<const char *>(m);
+        }
+        close(fd);
+    }
+    if (!mf.size) return set_error(CUTS_ERR_PARSE, "first line must hold the vertex count: " + path);
+    const char *p = mf.data, *end = mf.data + mf.size;
     const char *nl = static_cast<const char *>(std::memchr(p, '\n', size_t(end - p)));
     long long V;
     if (!parse_int(p, nl ? nl : end, V) || V < 0)
@@ -200,8 +238,9 @@ int load_graph_text(const std::string &path, HostGraph &g) {
     #pragma omp parallel for num_threads(T) schedule(static, 1)
     for (int t = 0; t < T; ++t) {
         const char *s = cut[t], *e = cut[t + 1];
-        auto &vs = ls[t];
-        auto &vd = ld[t];
+        // filled through locals and moved out at the end: vectors side by
+        // side in ls / ld would share cache lines between the threads
+        std::vector<uint32_t> vs, vd;
         vs.reserve(size_t(e - s) / 8);
         vd.reserve(size_t(e - s) / 8);
         while (s < e) {
@@ -217,19 +256,20 @@ int load_graph_text(const std::string &path, HostGraph &g) {
             }
             s = le + 1;
         }
+        ls[t] = std::move(vs);
+        ld[t] = std::move(vd);
     }
     for (int t = 0; t < T; ++t) {
         if (err[t] == 1) return set_error(CUTS_ERR_PARSE, "unparsable arc line in " + path);
         if (err[t] == 2) return set_error(CUTS_ERR_PARSE, "arc endpoint outside [0, V) in " + path);
     }
-    size_t total = 0;
-    for (auto &v : ls) total += v.size();
-    std::vector<uint32_t> src(total), dst(total);
-    size_t o = 0;
+    std::vector<size_t> at(size_t(T) + 1, 0);
+    for (int t = 0; t < T; ++t) at[t + 1] = at[t] + ls[t].size();
+    std::vector<uint32_t> src(at[T]), dst(at[T]);
+    #pragma omp parallel for num_threads(T) schedule(static, 1)
     for (int t = 0; t < T; ++t) {
-        std::copy(ls[t].begin(), ls[t].end(), src.begin() + o);
-        std::copy(ld[t].begin(), ld[t].end(), dst.begin() + o);
-        o += ls[t].size();
+        std::copy(ls[t].begin(), ls[t].end(), src.begin() + at[t]);
+        std::copy(ld[t].begin(), ld[t].end(), dst.begin() + at[t]);
         std::vector<uint32_t>().swap(ls[t]);
         std::vector<uint32_t>().swap(ld[t]);
     }

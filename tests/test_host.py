@@ -118,6 +118,35 @@ def test_loader_matches_reference_loader_on_random_files(tmp_path):
         assert not sym and io.tolist() == want["in_off"] and ia.tolist() == want["in_adj"]
 
 
+def test_loader_symmetry_finds_every_missing_reverse(tmp_path):
+    """The loader's symmetry check searches only the arcs going down in
+    (degree, id) order and compares the numbers going up and down: a graph
+    with self-loops is symmetric, the same graph without one arc (leaf to
+    hub, hub to leaf, between equal degrees) is not."""
+    h = cb.HostGraph.chung_lu(2000, 6000, 2.1, 2.0, 150.0, seed=21)
+    oo, oa, _, _ = h.csr()
+    src = np.repeat(np.arange(h.n), np.diff(oo).astype(np.int64))
+    deg = np.diff(oo)
+    hub = int(np.argmax(deg))
+    nb = oa[oo[hub]:oo[hub + 1]]
+    leaf = int(nb[np.argmin(deg[nb])])
+    same = next((u, int(v)) for u in range(h.n) for v in oa[oo[u]:oo[u + 1]] if deg[v] == deg[u] and v != u)
+    loops = np.arange(0, h.n, 5)
+
+    def load(drop):
+        keep = ~((src == drop[0]) & (oa == drop[1])) if drop else np.ones(len(oa), bool)
+        s = np.concatenate([src[keep], loops])
+        d = np.concatenate([oa[keep], loops])
+        p = str(tmp_path / "g.txt")
+        with open(p, "w") as f:
+            f.write(f"{h.n}\n" + "".join(f"{a}\t{b}\n" for a, b in zip(s, d)))
+        return cb.HostGraph.load(p).info()[2]
+
+    assert load(None) is True
+    for drop in [(hub, leaf), (leaf, hub), same, same[::-1]]:
+        assert load(drop) is False, drop
+
+
 @pytest.mark.parametrize("text,code", [
     ("", cb.ERR_PARSE),
     ("x\n0\t1\n", cb.ERR_PARSE),
